@@ -1,0 +1,398 @@
+"""Benchmark of the B200 CSR SpGEMM hot path: C = A*A on the power-law graph
+matrix (n = 1,000,000 rows, row degree Zipf(2.0) on [1, 4700], preferential-
+attachment columns, values U(0, 1], seeded), FP64 values.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one full product through the library's C ABI (spgemm_csr_f64, which
+allocates C like the reference's proposal(); C is released after the step, as
+the reference's `measure` lambda does).  value = 2 * NIP / step time (GFLOPS),
+inputs resident in HBM, L2 flushed between steps (256 MB write, outside the
+step events).  e2e = the same metric through the host-buffer entry point
+(spgemm_csr_host_f64): pinned host inputs copied in, C copied back, per step.
+
+--impl reference times the CPU restatement of the path (the reference has no
+CPU SpGEMM of its own) on this machine's host cores.
+
+Multi-GPU: replicas.  Every rank multiplies its own copy of the workload on its
+own GPU (the path has no exchange step); value = all ranks' FLOPs / the max
+over ranks of the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "C=A*A GFLOPS (2*NIP/s), power-law n=1e6 FP64"
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--dtype", choices=["f64", "f32"], default="f64")
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--exponent", type=float, default=2.0)
+    ap.add_argument("--cap", type=int, default=4700)
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--out", type=str, default="")
+    return ap.parse_args()
+
+
+def workload(args):
+    from gpuspgemm_b200 import generators as G
+    A = G.power_law(args.n, args.exponent, args.cap, seed=args.seed)
+    if args.dtype == "f32":
+        A = A.astype(np.float32)
+    return A
+
+
+def config_of(args, A, nip, nnz_c):
+    return {
+        "workload": f"power-law graph C=A*A, n={A.m}, Zipf({args.exponent}) degree cap "
+                    f"{args.cap}, preferential-attachment columns, seed {args.seed}",
+        "m": A.m, "nnz_A": A.nnz, "nip": nip, "nnz_C": nnz_c,
+        "value_dtype": args.dtype,
+        "l2": "flushed between steps (256 MB write outside the step events)",
+        "parallelism": f"replicas x{args.gpus}",
+    }
+
+
+# ---- algorithmic bytes (compulsory traffic) --------------------------------
+
+def rows_bytes(A, rows, nnz_c_rows, s, numeric, write_c):
+    """Compulsory bytes of a kernel over `rows` of C = A*A: the rows of A
+    (rpt pair, col [+ val]), each distinct B row they touch once (rpt pair,
+    col [+ val]), and the C output (nnz count, or rpt pair + col + val)."""
+    if rows.size == 0:
+        return 0
+    deg = np.diff(A.rpt)
+    starts = A.rpt[rows]
+    lens = deg[rows]
+    idx = np.repeat(starts - np.concatenate([[0], np.cumsum(lens)[:-1]]), lens) + \
+        np.arange(lens.sum())
+    cols = np.unique(A.col[idx])
+    per = 4 + (s if numeric else 0)
+    b = 8 * rows.size + per * int(lens.sum())
+    b += 8 * cols.size + per * int(deg[cols].sum())
+    if write_c:
+        b += 8 * rows.size + (4 + s) * int(nnz_c_rows.sum())
+    else:
+        b += 4 * rows.size
+    return int(b)
+
+
+def bin_rows(keys, limits, min_bin=0):
+    b = np.searchsorted(np.asarray(limits, dtype=np.int64), keys, side="left")
+    b = np.maximum(b, min_bin)
+    return b
+
+
+# ---- clocks -----------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---- the reference arm: CPU restatement on the host cores -------------------
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    import oracle
+    A = workload(args)
+    dt = np.float64 if args.dtype == "f64" else np.float32
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    nip = oracle.nip(A, A)
+    C = None
+    for _ in range(args.warmup):
+        C = oracle.spgemm(A, A, dt)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        C = oracle.spgemm(A, A, dt)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    gflops = 2.0 * nip * args.steps / total / 1e9
+    line = {
+        "metric": METRIC, "value": gflops, "unit": "GFLOPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": args.dtype, "data": "synthetic (seeded generator)",
+        "config": config_of(args, A, nip, C.nnz if C is not None else None),
+        "impl": "reference",
+        "cpu_baseline": {"value": gflops, "unit": "GFLOPS", "cores": threads, "kind": "port",
+                         "sample": "the full workload per step (row-wise Gustavson, "
+                                   "OpenMP over rows; the reference has no CPU SpGEMM)"},
+        "e2e": {"value": gflops, "unit": "GFLOPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+# ---- our arm ----------------------------------------------------------------
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from gpuspgemm_b200 import _native as N
+    from gpuspgemm_b200.api import DeviceCSR, Handle, proposal, proposal_host
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    A = workload(args)
+    dA = DeviceCSR.from_host(A, dev)
+    h = Handle(local_rank)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    C = None
+    c_rpt = None
+    for _ in range(max(args.warmup, 1)):
+        C = proposal(dA, dA, h)
+        c_rpt = C.rpt.cpu().numpy()
+        del C
+    info = h.info()
+    nip = info["nip"]
+    nnz_c = info["nnz"]
+
+    h.set_option(N.OPT_PROFILE, 1)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    kernel_ms = {}
+    launches = 0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            starts[i].record(stream)
+            C = proposal(dA, dA, h)
+            ends[i].record(stream)
+            del C
+            for k in h.profile():
+                key = (k["phase"], k["bin"], k["name"])
+                kernel_ms.setdefault(key, []).append(k["ms"])
+                launches += 1
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    h.set_option(N.OPT_PROFILE, 0)
+
+    value = 2.0 * nip * args.steps * world / (total_ms / 1e3) / 1e9
+
+    # e2e through the host-buffer entry point, pinned inputs
+    pin = {k: torch.from_numpy(np.ascontiguousarray(getattr(A, k))).pin_memory()
+           for k in ("rpt", "col", "val")}
+    from gpuspgemm_b200.csr import HostCSR
+    Ap = HostCSR(A.m, A.n, pin["rpt"].numpy(), pin["col"].numpy(), pin["val"].numpy())
+    s_bytes = 8 if args.dtype == "f64" else 4
+    h2d = 2 * (4 * (A.m + 1) + (4 + s_bytes) * A.nnz)
+    d2h = 4 * (A.m + 1) + (4 + s_bytes) * nnz_c
+    Ch = proposal_host(Ap, Ap, h)  # warm (grows the input staging)
+    del Ch
+    e2e_ms = []
+    if world > 1:
+        dist.barrier()
+    for _ in range(args.e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        Ch = proposal_host(Ap, Ap, h)
+        torch.cuda.synchronize()
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+        del Ch
+    e2e_total = float(sum(e2e_ms))
+    if world > 1:
+        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = 2.0 * nip * args.e2e_steps * world / (e2e_total / 1e3) / 1e9
+
+    if rank != 0:
+        h.close()
+        return None
+
+    # roofline of the dominant kernel
+    avg = {k: float(np.mean(v)) for k, v in kernel_ms.items()}
+    dom = max(avg, key=avg.get)
+    phase, b, name = dom
+    # per-row NIP (numpy) and nnz (the library's own C.rpt) for the byte model
+    deg = np.diff(A.rpt).astype(np.int64)
+    contrib = deg[A.col]
+    nip_rows = np.zeros(A.m, dtype=np.int64)
+    nz = deg > 0
+    nip_rows[nz] = np.add.reduceat(contrib, A.rpt[:-1][nz])
+    nnz_rows = np.diff(c_rpt).astype(np.int64)
+    if phase == 3:
+        lim = h.ladder(1, s_bytes)
+        keys = nnz_rows
+        numeric, write_c = True, True
+    elif phase == 1:
+        lim = h.ladder(0)
+        keys = nip_rows
+        numeric, write_c = False, False
+    else:
+        lim, keys = None, None
+    if lim is not None:
+        bins = bin_rows(keys, lim)
+        rows = np.nonzero((keys > 0) & (bins == b))[0]
+        alg_bytes = rows_bytes(A, rows, nnz_rows[rows], s_bytes, numeric, write_c)
+    else:
+        alg_bytes = 8 * A.m  # binning passes: row pointers / keys in and out
+    peaks = json.loads(PEAKS_FILE.read_text()) if PEAKS_FILE.exists() else {}
+    peak = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
+    achieved = alg_bytes / (avg[dom] / 1e3) / 1e9
+    whole_bytes = rows_bytes(A, np.arange(A.m), nnz_rows, s_bytes, True, True)
+    step_ms_avg = total_ms / args.steps
+    roofline = {
+        "bound": "hbm", "kernel": name, "phase": int(phase), "bin": int(b),
+        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+        "peak_source": "MEASURED_PEAKS.json" if PEAKS_FILE.exists() else "fallback",
+        "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg[dom], "traffic": None,
+        "whole_product": {"alg_bytes": whole_bytes,
+                          "achieved_gbs": whole_bytes / (step_ms_avg / 1e3) / 1e9},
+    }
+    kernels = sorted(({"kernel": k[2], "phase": k[0], "bin": k[1], "avg_ms": avg[k],
+                       "share": avg[k] / max(step_ms_avg, 1e-9)} for k in avg),
+                     key=lambda r: -r["avg_ms"])
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle  # the CPU baseline leg: the oracle is timed, not used
+        threads = os.cpu_count() or 1
+        oracle.set_threads(threads)
+        dt = np.float64 if args.dtype == "f64" else np.float32
+        oracle.spgemm(A, A, dt)
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            oracle.spgemm(A, A, dt)
+            ts.append(time.perf_counter() - t0)
+        cpu = {"value": 2.0 * nip / float(np.median(ts)) / 1e9, "unit": "GFLOPS",
+               "cores": threads, "kind": "port",
+               "sample": "the full workload, median of 3 (row-wise Gustavson, OpenMP)"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "GFLOPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": args.dtype, "data": "synthetic (seeded generator)",
+        "config": config_of(args, A, nip, nnz_c),
+        "e2e": {"value": e2e_value, "unit": "GFLOPS", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_total / args.e2e_steps},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "gpu_launches": launches,
+        "kernels": kernels[:12],
+        "host_syncs_per_step": info["host_syncs"],
+    }
+    h.close()
+    return line
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank)
+    else:
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        line = run_ours(args, rank, world, local_rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    if line is not None:
+        s = json.dumps(line)
+        print(s, flush=True)
+        if args.out:
+            Path(args.out).write_text(s + "\n")
+
+
+if __name__ == "__main__":
+    main()

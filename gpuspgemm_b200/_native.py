@@ -1,0 +1,147 @@
+"""ctypes binding of the C ABI in ``include/spgemm.h`` (libspgemm_b200.so).
+
+Import fails loudly when the library has not been built: there is no CPU or
+PyTorch fallback behind this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libspgemm_b200.so"
+
+SPGEMM_OK = 0
+STATUS_NAMES = {
+    0: "SPGEMM_OK",
+    1: "SPGEMM_ERR_INVALID_ARG",
+    2: "SPGEMM_ERR_OOM",
+    3: "SPGEMM_ERR_UNSUPPORTED_DEVICE",
+    4: "SPGEMM_ERR_OVERFLOW",
+    5: "SPGEMM_ERR_TIMEOUT",
+    6: "SPGEMM_ERR_CUDA",
+    7: "SPGEMM_ERR_INTERNAL",
+}
+
+OPT_CHECKED = 1
+OPT_MIN_SYM_BIN = 2
+OPT_MIN_NUM_BIN = 3
+OPT_CLUSTER_SIZE = 4
+OPT_STREAMS = 5
+OPT_PROFILE = 6
+
+
+class CsrView(C.Structure):
+    _fields_ = [
+        ("m", C.c_int32),
+        ("n", C.c_int32),
+        ("nnz", C.c_int32),
+        ("rpt", C.c_void_p),
+        ("col", C.c_void_p),
+        ("val", C.c_void_p),
+    ]
+
+
+class CsrOut(C.Structure):
+    _fields_ = [
+        ("m", C.c_int32),
+        ("n", C.c_int32),
+        ("nnz", C.c_int32),
+        ("rpt", C.c_void_p),
+        ("col", C.c_void_p),
+        ("val", C.c_void_p),
+    ]
+
+
+class Info(C.Structure):
+    _fields_ = [
+        ("nip", C.c_int64),
+        ("nnz", C.c_int64),
+        ("max_row_nip", C.c_int32),
+        ("max_row_nnz", C.c_int32),
+        ("sym_bin_rows", C.c_int32 * 16),
+        ("num_bin_rows", C.c_int32 * 16),
+        ("sym_fail_rows", C.c_int32),
+        ("n_sym_bins", C.c_int32),
+        ("n_num_bins", C.c_int32),
+        ("host_syncs", C.c_int32),
+    ]
+
+
+class KernelTime(C.Structure):
+    _fields_ = [
+        ("name", C.c_char * 48),
+        ("phase", C.c_int32),
+        ("bin", C.c_int32),
+        ("rows", C.c_int32),
+        ("ms", C.c_float),
+    ]
+
+
+# name -> (restype, argtypes); must list every function spgemm.h declares
+SIGNATURES = {
+    "spgemm_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int]),
+    "spgemm_destroy": (C.c_int, [C.c_void_p]),
+    "spgemm_csr_f64": (C.c_int, [C.c_void_p, C.POINTER(CsrView), C.POINTER(CsrView),
+                                 C.POINTER(CsrOut), C.c_void_p]),
+    "spgemm_csr_f32": (C.c_int, [C.c_void_p, C.POINTER(CsrView), C.POINTER(CsrView),
+                                 C.POINTER(CsrOut), C.c_void_p]),
+    "spgemm_csr_free": (C.c_int, [C.POINTER(CsrOut), C.c_void_p]),
+    "spgemm_csr_host_f64": (C.c_int, [C.c_void_p, C.POINTER(CsrView), C.POINTER(CsrView),
+                                      C.POINTER(CsrOut), C.c_void_p]),
+    "spgemm_csr_host_f32": (C.c_int, [C.c_void_p, C.POINTER(CsrView), C.POINTER(CsrView),
+                                      C.POINTER(CsrOut), C.c_void_p]),
+    "spgemm_host_csr_free": (C.c_int, [C.POINTER(CsrOut)]),
+    "spgemm_get_nip": (C.c_int, [C.c_void_p, C.POINTER(CsrView), C.POINTER(CsrView),
+                                 C.POINTER(C.c_int64), C.c_void_p]),
+    "spgemm_last_info": (C.c_int, [C.c_void_p, C.POINTER(Info)]),
+    "spgemm_last_profile": (C.c_int, [C.c_void_p, C.POINTER(KernelTime), C.c_int32,
+                                      C.POINTER(C.c_int32)]),
+    "spgemm_set_option": (C.c_int, [C.c_void_p, C.c_int, C.c_int64]),
+    "spgemm_get_option": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]),
+    "spgemm_ladder_info": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int64)]),
+    "spgemm_last_error_string": (C.c_char_p, []),
+    "spgemm_status_string": (C.c_char_p, [C.c_int]),
+    "spgemm_abi_version": (C.c_int, []),
+}
+
+
+class SpgemmError(RuntimeError):
+    """Raised for a non-OK status; mirrors the reference's std::runtime_error
+    (src/libutils/include/utils/errors.cuh:11-22)."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.status_name = STATUS_NAMES.get(status, f"status {status}")
+        super().__init__(f"{self.status_name}: {message}")
+
+
+def load(path: Path = LIB_PATH) -> C.CDLL:
+    if not path.exists():
+        raise ImportError(
+            f"{path.name} is not built; run `python -m gpuspgemm_b200.build` "
+            "(the package has no CPU fallback)")
+    lib = C.CDLL(str(path))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.spgemm_abi_version() != 1:
+        raise ImportError("libspgemm_b200.so ABI version mismatch")
+    return lib
+
+
+_lib: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        _lib = load()
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != SPGEMM_OK:
+        msg = lib().spgemm_last_error_string().decode(errors="replace")
+        raise SpgemmError(status, msg)

@@ -1,0 +1,271 @@
+"""Python mirror of the reference's hot-path interface.
+
+Reference (geektrove/GPUSpGEMM)                      here
+--------------------------------------------------  ---------------------------------
+utils::DeviceCSR<T>            (csr.cuh:22-63)       DeviceCSR (torch CUDA tensors)
+HostCSR::to<Device>() / to<Host>() (csr.cuh:193-203) DeviceCSR.from_host / .to_host
+proposal::proposal<T>(A, B)    (proposal.cuh:85-124) proposal(A, B)
+utils::get_nip(A, B)           (nip.cuh:52-78)       get_nip(A, B)
+apps' convert + run + to<Host> (proposal.cu:15-26)   proposal_host(A, B)
+
+Everything calls the C ABI of libspgemm_b200.so (include/spgemm.h); errors
+raise SpgemmError like the reference's std::runtime_error.  PyTorch only
+provides device memory and streams here.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .csr import HostCSR
+
+try:
+    import torch
+except ImportError:  # pragma: no cover - torch is part of the runtime image
+    torch = None
+
+
+def _require_torch():
+    if torch is None or not torch.cuda.is_available():
+        raise RuntimeError("a CUDA device is required")
+
+
+class Handle:
+    """Owns one spgemm_handle_t (scratch, side streams, pinned staging)."""
+
+    def __init__(self, device: int | None = None):
+        self._h = C.c_void_p()
+        dev = -1 if device is None else int(device)
+        N.check(N.lib().spgemm_create(C.byref(self._h), dev))
+
+    @property
+    def ptr(self) -> C.c_void_p:
+        if not self._h:
+            raise RuntimeError("handle is closed")
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            N.lib().spgemm_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_option(self, option: int, value: int) -> None:
+        N.check(N.lib().spgemm_set_option(self.ptr, option, int(value)))
+
+    def get_option(self, option: int) -> int:
+        v = C.c_int64()
+        N.check(N.lib().spgemm_get_option(self.ptr, option, C.byref(v)))
+        return int(v.value)
+
+    def info(self) -> dict:
+        inf = N.Info()
+        N.check(N.lib().spgemm_last_info(self.ptr, C.byref(inf)))
+        return {
+            "nip": int(inf.nip),
+            "nnz": int(inf.nnz),
+            "max_row_nip": int(inf.max_row_nip),
+            "max_row_nnz": int(inf.max_row_nnz),
+            "sym_bin_rows": list(inf.sym_bin_rows)[: inf.n_sym_bins],
+            "num_bin_rows": list(inf.num_bin_rows)[: inf.n_num_bins],
+            "sym_fail_rows": int(inf.sym_fail_rows),
+            "host_syncs": int(inf.host_syncs),
+        }
+
+    def profile(self) -> list[dict]:
+        """Per-launch event-timed durations of the last product
+        (requires set_option(OPT_PROFILE, 1))."""
+        cnt = C.c_int32()
+        N.check(N.lib().spgemm_last_profile(self.ptr, None, 0, C.byref(cnt)))
+        arr = (N.KernelTime * max(cnt.value, 1))()
+        N.check(N.lib().spgemm_last_profile(self.ptr, arr, cnt.value, C.byref(cnt)))
+        return [{"name": k.name.decode(), "phase": k.phase, "bin": k.bin, "rows": k.rows,
+                 "ms": k.ms} for k in arr[: cnt.value]]
+
+    def ladder(self, which: int, dtype_bytes: int = 8) -> list[int]:
+        nb = C.c_int()
+        lim = (C.c_int64 * 16)()
+        N.check(N.lib().spgemm_ladder_info(self.ptr, which, dtype_bytes, C.byref(nb), lim))
+        return list(lim)[: nb.value]
+
+
+_local = threading.local()
+
+
+def default_handle() -> Handle:
+    """One handle per host thread (the C ABI's threading rule)."""
+    h = getattr(_local, "handle", None)
+    if h is None:
+        h = Handle()
+        _local.handle = h
+    return h
+
+
+class _LibraryArray:
+    """A device array allocated by the library, exposed through
+    __cuda_array_interface__ so torch can wrap it without a copy."""
+
+    def __init__(self, owner: "_ResultOwner", ptr: int, n: int, typestr: str):
+        self._owner = owner
+        self.__cuda_array_interface__ = {
+            "shape": (n,),
+            "typestr": typestr,
+            "data": (ptr, False),
+            "version": 2,
+        }
+
+
+class _ResultOwner:
+    """Frees a library-allocated result (spgemm_csr_free) once no tensor
+    refers to it any more."""
+
+    def __init__(self, out: N.CsrOut):
+        self.out = out
+
+    def __del__(self):
+        try:
+            N.lib().spgemm_csr_free(C.byref(self.out), None)
+        except Exception:
+            pass
+
+
+@dataclass
+class DeviceCSR:
+    """CSR on the device: int32 rpt/col and float32/float64 val torch tensors."""
+
+    m: int
+    n: int
+    rpt: "torch.Tensor"
+    col: "torch.Tensor"
+    val: "torch.Tensor"
+
+    @property
+    def nnz(self) -> int:
+        return int(self.col.numel())
+
+    @property
+    def dtype(self):
+        return self.val.dtype
+
+    @staticmethod
+    def from_host(a: HostCSR, device="cuda", pin: bool = False) -> "DeviceCSR":
+        _require_torch()
+
+        def t(x):
+            ht = torch.from_numpy(np.ascontiguousarray(x))
+            if pin:
+                ht = ht.pin_memory()
+            return ht.to(device, non_blocking=pin)
+
+        return DeviceCSR(a.m, a.n, t(a.rpt), t(a.col), t(a.val))
+
+    def to_host(self) -> HostCSR:
+        return HostCSR(self.m, self.n, self.rpt.cpu().numpy(), self.col.cpu().numpy(),
+                       self.val.cpu().numpy())
+
+    def view(self) -> N.CsrView:
+        for name, x, dt in (("rpt", self.rpt, torch.int32), ("col", self.col, torch.int32)):
+            if x.dtype != dt or not x.is_cuda or not x.is_contiguous():
+                raise TypeError(f"{name} must be a contiguous int32 CUDA tensor")
+        if self.val.dtype not in (torch.float32, torch.float64) or not self.val.is_cuda:
+            raise TypeError("val must be a float32 or float64 CUDA tensor")
+        return N.CsrView(self.m, self.n, self.nnz, self.rpt.data_ptr(),
+                         self.col.data_ptr() if self.nnz else None,
+                         self.val.data_ptr() if self.nnz else None)
+
+
+def _stream_ptr(stream) -> int | None:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return stream.cuda_stream or None
+
+
+def proposal(A: DeviceCSR, B: DeviceCSR, handle: Handle | None = None,
+             stream=None) -> DeviceCSR:
+    """C = A * B on the device (reference proposal::proposal, proposal.cuh:85-124).
+
+    A and B must share a dtype (float32 or float64), have int32 indices and
+    sorted, duplicate-free columns per row.  Synchronous on return.
+    """
+    _require_torch()
+    if A.dtype != B.dtype:
+        raise TypeError("A and B must have the same value dtype")
+    h = handle or default_handle()
+    out = N.CsrOut()
+    va, vb = A.view(), B.view()
+    fn = N.lib().spgemm_csr_f64 if A.dtype == torch.float64 else N.lib().spgemm_csr_f32
+    N.check(fn(h.ptr, C.byref(va), C.byref(vb), C.byref(out), _stream_ptr(stream)))
+    return _wrap_result(out, A.dtype)
+
+
+def _wrap_result(out: N.CsrOut, dtype) -> DeviceCSR:
+    owner = _ResultOwner(out)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    vt = "<f8" if dtype == torch.float64 else "<f4"
+    rpt = torch.as_tensor(_LibraryArray(owner, out.rpt, out.m + 1, "<i4"), device=dev)
+    if out.nnz > 0:
+        col = torch.as_tensor(_LibraryArray(owner, out.col, out.nnz, "<i4"), device=dev)
+        val = torch.as_tensor(_LibraryArray(owner, out.val, out.nnz, vt), device=dev)
+    else:
+        col = torch.empty(0, dtype=torch.int32, device=dev)
+        val = torch.empty(0, dtype=dtype, device=dev)
+    return DeviceCSR(out.m, out.n, rpt, col, val)
+
+
+def _host_view(a: HostCSR) -> tuple[N.CsrView, list]:
+    keep = [np.ascontiguousarray(a.rpt, dtype=np.int32),
+            np.ascontiguousarray(a.col, dtype=np.int32),
+            np.ascontiguousarray(a.val)]
+    v = N.CsrView(a.m, a.n, a.nnz, keep[0].ctypes.data, keep[1].ctypes.data,
+                  keep[2].ctypes.data)
+    return v, keep
+
+
+def proposal_host(A: HostCSR, B: HostCSR, handle: Handle | None = None,
+                  stream=None) -> HostCSR:
+    """C = A * B from host operands to a host result through the C ABI's host
+    entry point (copies inside the call, like the apps' convert/run/to<Host>)."""
+    if A.val.dtype != B.val.dtype:
+        raise TypeError("A and B must have the same value dtype")
+    h = handle or default_handle()
+    va, ka = _host_view(A)
+    vb, kb = _host_view(B)
+    out = N.CsrOut()
+    f64 = A.val.dtype == np.float64
+    fn = N.lib().spgemm_csr_host_f64 if f64 else N.lib().spgemm_csr_host_f32
+    sp = _stream_ptr(stream) if torch is not None and torch.cuda.is_available() else None
+    N.check(fn(h.ptr, C.byref(va), C.byref(vb), C.byref(out), sp))
+    m, n = int(out.m), int(out.n)
+    try:
+        vdt = np.float64 if f64 else np.float32
+        rpt = np.ctypeslib.as_array(C.cast(out.rpt, C.POINTER(C.c_int32)), (out.m + 1,)).copy()
+        if out.nnz > 0:
+            col = np.ctypeslib.as_array(C.cast(out.col, C.POINTER(C.c_int32)), (out.nnz,)).copy()
+            cval = C.cast(out.val, C.POINTER(C.c_double if f64 else C.c_float))
+            val = np.ctypeslib.as_array(cval, (out.nnz,)).astype(vdt, copy=True)
+        else:
+            col = np.zeros(0, np.int32)
+            val = np.zeros(0, vdt)
+    finally:
+        N.lib().spgemm_host_csr_free(C.byref(out))
+    del ka, kb
+    return HostCSR(m, n, rpt, col, val)
+
+
+def get_nip(A: DeviceCSR, B: DeviceCSR, handle: Handle | None = None, stream=None) -> int:
+    """Total intermediate products (reference utils::get_nip, nip.cuh:52-78)."""
+    h = handle or default_handle()
+    v = C.c_int64()
+    va, vb = A.view(), B.view()
+    N.check(N.lib().spgemm_get_nip(h.ptr, C.byref(va), C.byref(vb), C.byref(v),
+                                   _stream_ptr(stream)))
+    return int(v.value)

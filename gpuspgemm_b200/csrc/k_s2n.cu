@@ -1,0 +1,271 @@
+// Symbolic phase 2 fused with the numeric phase, one kernel per row bin
+// (key = nnz of the row, known exactly after the count phase and the scan).
+//
+// For every row the kernel
+//   1. hashes the row's column keys into a shared-memory table
+//      (sym2.cuh:84-101, 163-191),
+//   2. sorts the keys and stores them as C.col[rpt[row] ...]
+//      (sym2.cuh:104-120, 194-210),
+//   3. accumulates c_ij += a_ik * b_kj with a binary search of the sorted keys
+//      and a shared-memory atomic add (num.cuh:104-116, 162-182),
+//   4. stores C.val.
+// The reference runs 2 and 3 as separate phases with a second binning in
+// between (proposal.cuh:59-73), re-reading C.col from global memory; here the
+// sorted keys stay in shared memory.  The results are the same: the sorted
+// key list is unique, and each value is the sum of the same rounded products.
+#include <cooperative_groups.h>
+
+#include "cta.cuh"
+#include "kernels.hpp"
+
+namespace cg = cooperative_groups;
+
+namespace b200 {
+
+namespace {
+
+template<typename V>
+__device__ __forceinline__ V ldv(const void* base, int i) {
+    return __ldg(static_cast<const V*>(base) + i);
+}
+
+template<typename V, int G, int THREADS, int T, int CAP>
+__global__ __launch_bounds__(THREADS) void k_s2n_team(ProductArgs p) {
+    constexpr int R = THREADS / G;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* s_vals = reinterpret_cast<V*>(smem_raw);
+    int32_t* s_keys = reinterpret_cast<int32_t*>(smem_raw + sizeof(V) * R * CAP);
+    const int team = threadIdx.x / G;
+    const int lane = team_lane<G>();
+    const unsigned mask = team_mask<G>();
+    const int rid = blockIdx.x * R + team;
+    if (rid >= p.nrows) return;
+    int32_t* keys = s_keys + team * T;
+    V* vals = s_vals + team * CAP;
+    const int row = p.rows[rid];
+    const int c0 = p.c_rpt[row];
+    const int nnz = p.c_rpt[row + 1] - c0;
+    if (nnz > CAP) {
+        if (lane == 0) report(p.status, kStCapacity, row, nnz);
+        return;
+    }
+    for (int i = lane; i < T; i += G) keys[i] = kEmpty;
+    team_sync<G>(mask);
+    const int a0 = p.a_rpt[row];
+    const int a1 = p.a_rpt[row + 1];
+    team_for_products<G>(p.a_col, p.b_rpt, a0, a1, [&](int qb, int) {
+        table_insert(keys, T, __ldg(p.b_col + qb), p.status, row);
+    });
+    team_sync<G>(mask);
+    team_bitonic_sort<G>(keys, T, mask, lane);
+    for (int i = lane; i < nnz; i += G) {
+        p.c_col[c0 + i] = keys[i];
+        vals[i] = V(0);
+    }
+    team_sync<G>(mask);
+    team_for_products<G>(p.a_col, p.b_rpt, a0, a1, [&](int qb, int ai) {
+        const int32_t key = __ldg(p.b_col + qb);
+        const int pos = lower_bound_present(keys, nnz, key);
+        atomicAdd(vals + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
+    });
+    team_sync<G>(mask);
+    V* out = static_cast<V*>(p.c_val) + c0;
+    for (int i = lane; i < nnz; i += G) out[i] = vals[i];
+}
+
+template<typename V, int THREADS, int T, int CAP>
+struct CtaLayout {
+    static constexpr int P = next_pow2(CAP);
+    static constexpr int K = T > P ? T : P;
+    static constexpr size_t vals_bytes = sizeof(V) * CAP;
+    static constexpr size_t keys_bytes = sizeof(int32_t) * K;
+    static constexpr size_t bytes = vals_bytes + keys_bytes + sizeof(CtaScratch<THREADS>);
+};
+
+template<typename V, int THREADS, int T, int CAP>
+__global__ __launch_bounds__(THREADS) void k_s2n_cta(ProductArgs p) {
+    using L = CtaLayout<V, THREADS, T, CAP>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* vals = reinterpret_cast<V*>(smem_raw);
+    int32_t* keys = reinterpret_cast<int32_t*>(smem_raw + L::vals_bytes);
+    auto& sc = *reinterpret_cast<CtaScratch<THREADS>*>(smem_raw + L::vals_bytes + L::keys_bytes);
+    const int row = p.rows[blockIdx.x];
+    const int c0 = p.c_rpt[row];
+    const int nnz = p.c_rpt[row + 1] - c0;
+    if (nnz > CAP) {
+        if (threadIdx.x == 0) report(p.status, kStCapacity, row, nnz);
+        return;
+    }
+    for (int i = threadIdx.x; i < T; i += THREADS) keys[i] = kEmpty;
+    __syncthreads();
+    const int a0 = p.a_rpt[row];
+    const int a1 = p.a_rpt[row + 1];
+    cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int) {
+        table_insert(keys, T, __ldg(p.b_col + qb), p.status, row);
+    });
+    const int cnt = cta_compact<THREADS>(keys, T, sc.warp_tot);
+    if (cnt != nnz && threadIdx.x == 0) report(p.status, kStCapacity, row, cnt);
+    const int pn = next_pow2(nnz);
+    for (int i = nnz + threadIdx.x; i < pn; i += THREADS) keys[i] = kEmpty;
+    __syncthreads();
+    cta_bitonic_sort<THREADS>(keys, pn);
+    for (int i = threadIdx.x; i < nnz; i += THREADS) {
+        p.c_col[c0 + i] = keys[i];
+        vals[i] = V(0);
+    }
+    __syncthreads();
+    cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int ai) {
+        const int32_t key = __ldg(p.b_col + qb);
+        const int pos = lower_bound_present(keys, nnz, key);
+        atomicAdd(vals + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
+    });
+    V* out = static_cast<V*>(p.c_val) + c0;
+    for (int i = threadIdx.x; i < nnz; i += THREADS) out[i] = vals[i];
+}
+
+// Global bin: bitmap of B.n bits per row in flight; the set bits, read in
+// word order, ARE the sorted column list.  Values accumulate with global
+// atomics after a binary search of the row's C.col in global memory
+// (the reference's k_num_global, num.cuh:251-298).
+template<typename V, int THREADS>
+__global__ __launch_bounds__(THREADS) void k_s2n_global(ProductArgs p) {
+    __shared__ CtaScratch<THREADS> sc;
+    uint32_t* bm = p.bitmaps + static_cast<int64_t>(blockIdx.x) * p.words;
+    for (int rid = blockIdx.x; rid < p.nrows; rid += gridDim.x) {
+        const int row = p.rows[rid];
+        const int c0 = p.c_rpt[row];
+        const int nnz = p.c_rpt[row + 1] - c0;
+        const int a0 = p.a_rpt[row];
+        const int a1 = p.a_rpt[row + 1];
+        for (int64_t i = threadIdx.x; i < p.words; i += THREADS) bm[i] = 0u;
+        __syncthreads();
+        cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int) {
+            const int32_t key = __ldg(p.b_col + qb);
+            atomicOr(bm + (key >> 5), 1u << (key & 31));
+        });
+        int32_t* cols = p.c_col + c0;
+        int base = 0;
+        for (int64_t c = 0; c < p.words; c += THREADS) {
+            const int64_t wi = c + threadIdx.x;
+            uint32_t w = wi < p.words ? bm[wi] : 0u;
+            const int cnt = __popc(w);
+            const int inc = block_inclusive_scan<THREADS>(cnt, sc.warp_tot);
+            int pos = base + inc - cnt;
+            while (w != 0u) {
+                const int b = __ffs(w) - 1;
+                if (pos < nnz) cols[pos] = static_cast<int32_t>(wi * 32 + b);
+                pos++;
+                w &= w - 1u;
+            }
+            base += sc.warp_tot[THREADS / kWarp - 1];
+            __syncthreads();
+        }
+        if (base != nnz && threadIdx.x == 0) report(p.status, kStCapacity, row, base);
+        V* out = static_cast<V*>(p.c_val) + c0;
+        for (int i = threadIdx.x; i < nnz; i += THREADS) out[i] = V(0);
+        __syncthreads();
+        cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int ai) {
+            const int32_t key = __ldg(p.b_col + qb);
+            const int pos = lower_bound_present(cols, nnz, key);
+            atomicAdd(out + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
+        });
+    }
+}
+
+template<typename V, int G, int THREADS, int T, int CAP>
+constexpr size_t team_smem() {
+    return (sizeof(V) * CAP + sizeof(int32_t) * T) * (THREADS / G);
+}
+
+template<typename V, int G, int THREADS, int T, int CAP>
+cudaError_t launch_team(const ProductArgs& p, cudaStream_t s) {
+    constexpr int R = THREADS / G;
+    const int grid = (p.nrows + R - 1) / R;
+    k_s2n_team<V, G, THREADS, T, CAP>
+        <<<grid, THREADS, team_smem<V, G, THREADS, T, CAP>(), s>>>(p);
+    return cudaGetLastError();
+}
+
+template<typename V, int THREADS, int T, int CAP>
+cudaError_t launch_cta(const ProductArgs& p, cudaStream_t s) {
+    k_s2n_cta<V, THREADS, T, CAP>
+        <<<p.nrows, THREADS, CtaLayout<V, THREADS, T, CAP>::bytes, s>>>(p);
+    return cudaGetLastError();
+}
+
+template<typename V, int THREADS>
+cudaError_t launch_global(const ProductArgs& p, cudaStream_t s) {
+    const int grid = p.nrows < p.nmaps ? p.nrows : p.nmaps;
+    k_s2n_global<V, THREADS><<<grid, THREADS, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+template<typename V>
+struct S2nLadder {
+    static const BinLauncher entries[];
+    static const int count;
+};
+
+#define B200_S2N_LADDER(V)                                                                    \
+    template<>                                                                                \
+    const BinLauncher S2nLadder<V>::entries[] = {                                             \
+        {BinKind::Team, 12, 64, 256, team_smem<V, 4, 256, 16, 12>(), "s2n_team4_t16",         \
+         launch_team<V, 4, 256, 16, 12>},                                                     \
+        {BinKind::Team, 48, 32, 256, team_smem<V, 8, 256, 64, 48>(), "s2n_team8_t64",         \
+         launch_team<V, 8, 256, 64, 48>},                                                     \
+        {BinKind::Team, 192, 16, 256, team_smem<V, 16, 256, 256, 192>(), "s2n_team16_t256",   \
+         launch_team<V, 16, 256, 256, 192>},                                                  \
+        {BinKind::Team, 768, 8, 256, team_smem<V, 32, 256, 1024, 768>(), "s2n_team32_t1024",  \
+         launch_team<V, 32, 256, 1024, 768>},                                                 \
+        {BinKind::Cta, 3072, 1, 256, CtaLayout<V, 256, 4096, 3072>::bytes, "s2n_cta256_t4096", \
+         launch_cta<V, 256, 4096, 3072>},                                                     \
+        {BinKind::Cta, 12288, 1, 512, CtaLayout<V, 512, 16384, 12288>::bytes,                 \
+         "s2n_cta512_t16384", launch_cta<V, 512, 16384, 12288>},                              \
+        {BinKind::Cta, 16384, 1, 1024, CtaLayout<V, 1024, 20480, 16384>::bytes,               \
+         "s2n_cta1024_t20480", launch_cta<V, 1024, 20480, 16384>},                            \
+        {BinKind::Global, INT32_MAX, 1, 1024, 0, "s2n_global_bitmap", launch_global<V, 1024>}, \
+    };                                                                                        \
+    template<>                                                                                \
+    const int S2nLadder<V>::count = sizeof(S2nLadder<V>::entries) / sizeof(BinLauncher);
+
+B200_S2N_LADDER(double)
+B200_S2N_LADDER(float)
+#undef B200_S2N_LADDER
+
+template<typename V>
+cudaError_t prepare_one() {
+    cudaError_t e = cudaSuccess;
+#define B200_SMEM(kern, bytes)                                                            \
+    if (e == cudaSuccess)                                                                 \
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+                                 static_cast<int>(bytes));
+    B200_SMEM((k_s2n_team<V, 4, 256, 16, 12>), (team_smem<V, 4, 256, 16, 12>()));
+    B200_SMEM((k_s2n_team<V, 8, 256, 64, 48>), (team_smem<V, 8, 256, 64, 48>()));
+    B200_SMEM((k_s2n_team<V, 16, 256, 256, 192>), (team_smem<V, 16, 256, 256, 192>()));
+    B200_SMEM((k_s2n_team<V, 32, 256, 1024, 768>), (team_smem<V, 32, 256, 1024, 768>()));
+    B200_SMEM((k_s2n_cta<V, 256, 4096, 3072>), (CtaLayout<V, 256, 4096, 3072>::bytes));
+    B200_SMEM((k_s2n_cta<V, 512, 16384, 12288>), (CtaLayout<V, 512, 16384, 12288>::bytes));
+    B200_SMEM((k_s2n_cta<V, 1024, 20480, 16384>), (CtaLayout<V, 1024, 20480, 16384>::bytes));
+#undef B200_SMEM
+    return e;
+}
+
+}  // namespace
+
+int s2n_ladder_f64(const BinLauncher** out) {
+    *out = S2nLadder<double>::entries;
+    return S2nLadder<double>::count;
+}
+
+int s2n_ladder_f32(const BinLauncher** out) {
+    *out = S2nLadder<float>::entries;
+    return S2nLadder<float>::count;
+}
+
+cudaError_t s2n_prepare() {
+    cudaError_t e = prepare_one<double>();
+    if (e == cudaSuccess) e = prepare_one<float>();
+    return e;
+}
+
+}  // namespace b200

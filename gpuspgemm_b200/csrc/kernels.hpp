@@ -1,0 +1,111 @@
+// Host-visible interface between the orchestration (spgemm.cu) and the kernel
+// translation units.  Plain structs only; no torch types anywhere.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace b200 {
+
+struct DevStatus;
+
+constexpr int kMaxBins = 16;
+
+// Row-bin ladder: row r (key k > 0) goes to the first bin b with k <= limit[b],
+// and at least to bin min_bin.  Rows with key 0 have an empty C row and join no
+// bin.  The reference's find_bin (binning.cuh:26-35) does the same linear walk
+// over its RANGES tables (parameters.cuh:53-64, 85-95, 127-144).
+struct Ladder {
+    int32_t nb;
+    int32_t min_bin;
+    int32_t limit[kMaxBins];
+};
+
+// Results of a binning pass, mirrored to pinned host memory in one copy.
+struct Plan {
+    int64_t total_key;        // sum of keys (total NIP, or total nnz)
+    int32_t max_key;          // max key over rows
+    int32_t overflow;         // a sum left int32 range
+    int32_t bin_size[kMaxBins];
+    int32_t bin_off[kMaxBins];
+};
+
+// Everything a per-bin kernel needs.  Values are passed as void* and cast by
+// the typed launcher.
+struct ProductArgs {
+    const int32_t* a_rpt;
+    const int32_t* a_col;
+    const void* a_val;
+    const int32_t* b_rpt;
+    const int32_t* b_col;
+    const void* b_val;
+    int32_t n_cols;         // B.n
+    int32_t* c_rpt;         // NIP / nnz per row (symbolic) or row pointer (fill)
+    int32_t* c_col;
+    void* c_val;
+    DevStatus* status;
+    const int32_t* rows;    // this bin's rows
+    int32_t nrows;
+    // global-bin scratch: nmaps bitmaps of `words` 32-bit words each
+    uint32_t* bitmaps;
+    int64_t words;
+    int32_t nmaps;
+    // cluster bins
+    int32_t cluster;        // CTAs per cluster
+    int32_t* fail_rows;     // rows that spilled out of a cluster table
+    int32_t* fail_count;
+};
+
+enum class BinKind : int { Team = 0, Cta = 1, Cluster = 2, Global = 3 };
+
+struct BinLauncher {
+    BinKind kind;
+    int32_t limit;          // largest key the kernel accepts
+    int32_t rows_per_cta;   // 1 for CTA/cluster/global kinds
+    int32_t threads;
+    size_t smem;            // dynamic shared memory per CTA
+    const char* name;
+    cudaError_t (*launch)(const ProductArgs&, cudaStream_t);
+};
+
+// Symbolic count ladder (key = NIP of the row).
+int sym1_ladder(const BinLauncher** out);
+// Fused fill + sort + numeric ladder (key = nnz of the row), per value type.
+int s2n_ladder_f64(const BinLauncher** out);
+int s2n_ladder_f32(const BinLauncher** out);
+// One-time per-device attribute setup (dynamic smem opt-in) for all kernels.
+cudaError_t sym1_prepare();
+cudaError_t s2n_prepare();
+
+// ---- binning / scan kernels (k_bin.cu) ------------------------------------
+constexpr int kBinThreads = 256;
+constexpr int kBinRowsPerCta = 1024;
+
+inline int bin_ctas(int32_t m) { return (m + kBinRowsPerCta - 1) / kBinRowsPerCta; }
+
+// Pass 1 (key = NIP): writes nip[r] into c_rpt[r], per-CTA bin histograms and
+// the plan's total / max.
+cudaError_t launch_nip_hist(const int32_t* a_rpt, const int32_t* a_col, const int32_t* b_rpt,
+                            int32_t m, int32_t* c_rpt, int32_t* hist, Plan* plan,
+                            DevStatus* st, const Ladder& lad, cudaStream_t s);
+// Pass 1' (key = nnz already in c_rpt): per-CTA sums and bin histograms.
+cudaError_t launch_nnz_hist(const int32_t* c_rpt, int32_t m, int32_t* hist, int64_t* cta_sum,
+                            Plan* plan, const Ladder& lad, cudaStream_t s);
+// Pass 2: exclusive offsets of the per-CTA histograms (and of cta_sum when
+// given), bin sizes/offsets into the plan.
+cudaError_t launch_bin_offsets(int32_t* hist, int32_t nctas, int64_t* cta_sum, Plan* plan,
+                               const Ladder& lad, cudaStream_t s);
+// Pass 3: stable scatter of row ids into bins.  When `scan` is set, also
+// rewrites c_rpt[0..m] as the exclusive scan of the nnz it holds.
+cudaError_t launch_bin_scatter(int32_t* c_rpt, int32_t m, const int32_t* hist_off,
+                               const int64_t* cta_off, int32_t* bins, const Plan* plan,
+                               const Ladder& lad, bool scan, cudaStream_t s);
+// Operand validation (checked mode).
+cudaError_t launch_check_csr(const int32_t* rpt, const int32_t* col, int32_t m, int32_t n,
+                             int32_t nnz, DevStatus* st, cudaStream_t s);
+// Total NIP only (spgemm_get_nip).
+cudaError_t launch_total_nip(const int32_t* a_rpt, const int32_t* a_col, const int32_t* b_rpt,
+                             int32_t m, long long* out, cudaStream_t s);
+
+}  // namespace b200

@@ -1,0 +1,824 @@
+// Host orchestration of the B200 CSR SpGEMM and its C ABI (include/spgemm.h).
+//
+// One product (reference: proposal_inner, proposal.cuh:26-80):
+//   count pass      NIP per row -> per-CTA histograms -> offsets -> stable
+//                   scatter of rows into count bins            [host sync 1]
+//   sym1            one kernel per non-empty count bin, heavy bins first,
+//                   spread over side streams; cluster-bin spills go to the
+//                   global bin in stream order (no host round-trip)
+//   scan pass       nnz histograms -> offsets -> scatter + exclusive scan of
+//                   C.rpt                                         [host sync 2]
+//   fill+numeric    allocate C.col / C.val, one fused kernel per non-empty bin
+//                   [final sync]
+// The reference synchronises with the host after every binning step and
+// creates/destroys its streams and scratch in every call (setup.cuh:164-165,
+// cleanup.cuh:15-31); here streams, events and scratch live in the handle.
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/spgemm.h"
+#include "common.cuh"
+#include "kernels.hpp"
+
+namespace b200 {
+namespace {
+
+thread_local std::string g_last_error;
+
+spgemm_status fail(spgemm_status st, const std::string& msg) {
+    g_last_error = msg;
+    return st;
+}
+
+spgemm_status cuda_fail(cudaError_t e, const char* what) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? SPGEMM_ERR_OOM : SPGEMM_ERR_CUDA;
+}
+
+#define B200_TRY(expr)                                                \
+    do {                                                              \
+        cudaError_t e_ = (expr);                                      \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #expr);           \
+    } while (0)
+
+constexpr int kMaxSide = 8;
+// Bitmap pool budget of the global bins (bytes).
+constexpr int64_t kBitmapBudget = int64_t(1) << 30;
+
+struct Scratch {
+    DevStatus* status;
+    Plan* plan1;
+    Plan* plan2;
+    int32_t* hist1;
+    int32_t* hist2;
+    int64_t* cta_sum;
+    int32_t* bins1;
+    int32_t* bins2;
+    int32_t* fail_rows;
+    int32_t* fail_count;
+};
+
+struct ProfRec {
+    const char* name;
+    int32_t phase;
+    int32_t bin;
+    int32_t rows;
+    cudaEvent_t a;
+    cudaEvent_t b;
+};
+
+// Pinned host mirror of the device-side plan words, copied in one transfer.
+struct HostMirror {
+    Plan plan;
+    DevStatus status;
+    int32_t fail_count;
+    int32_t pad[3];
+};
+
+}  // namespace
+}  // namespace b200
+
+struct spgemm_handle_s {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t side[b200::kMaxSide] = {};
+    cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_join[b200::kMaxSide] = {};
+    int nside = 4;
+    // scratch (grown, never shrunk)
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    uint32_t* bitmaps = nullptr;
+    size_t bitmap_bytes = 0;
+    b200::HostMirror* mirror = nullptr;  // pinned
+    // host-operand staging on the device
+    void* in_buf = nullptr;
+    size_t in_bytes = 0;
+    // options
+    int checked = 0;
+    int min_sym_bin = -1;
+    int min_num_bin = -1;
+    int cluster = 4;
+    int profile = 0;
+    spgemm_info info = {};
+    // profiling: an event pair per launch, resolved after the final sync
+    std::vector<b200::ProfRec> prof;
+    std::vector<cudaEvent_t> prof_events;
+    std::vector<spgemm_kernel_time> prof_done;
+};
+
+namespace b200 {
+namespace {
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s) {
+    const size_t nctas = static_cast<size_t>(bin_ctas(m > 0 ? m : 1));
+    const size_t mm = static_cast<size_t>(m > 0 ? m : 1);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = align_up(off + bytes, 256);
+        return o;
+    };
+    const size_t o_status = take(sizeof(DevStatus));
+    const size_t o_plan1 = take(sizeof(Plan));
+    const size_t o_plan2 = take(sizeof(Plan));
+    const size_t o_fail_count = take(sizeof(int32_t));
+    const size_t o_hist1 = take(sizeof(int32_t) * kMaxBins * nctas);
+    const size_t o_hist2 = take(sizeof(int32_t) * kMaxBins * nctas);
+    const size_t o_sum = take(sizeof(int64_t) * nctas);
+    const size_t o_bins1 = take(sizeof(int32_t) * mm);
+    const size_t o_bins2 = take(sizeof(int32_t) * mm);
+    const size_t o_fail = take(sizeof(int32_t) * mm);
+    if (off > h->scratch_bytes) {
+        if (h->scratch != nullptr) {
+            B200_TRY(cudaDeviceSynchronize());
+            B200_TRY(cudaFree(h->scratch));
+            h->scratch = nullptr;
+            h->scratch_bytes = 0;
+        }
+        const size_t bytes = off + off / 4;
+        B200_TRY(cudaMalloc(&h->scratch, bytes));
+        h->scratch_bytes = bytes;
+    }
+    char* b = static_cast<char*>(h->scratch);
+    s->status = reinterpret_cast<DevStatus*>(b + o_status);
+    s->plan1 = reinterpret_cast<Plan*>(b + o_plan1);
+    s->plan2 = reinterpret_cast<Plan*>(b + o_plan2);
+    s->fail_count = reinterpret_cast<int32_t*>(b + o_fail_count);
+    s->hist1 = reinterpret_cast<int32_t*>(b + o_hist1);
+    s->hist2 = reinterpret_cast<int32_t*>(b + o_hist2);
+    s->cta_sum = reinterpret_cast<int64_t*>(b + o_sum);
+    s->bins1 = reinterpret_cast<int32_t*>(b + o_bins1);
+    s->bins2 = reinterpret_cast<int32_t*>(b + o_bins2);
+    s->fail_rows = reinterpret_cast<int32_t*>(b + o_fail);
+    return SPGEMM_OK;
+}
+
+spgemm_status ensure_bitmaps(spgemm_handle_s* h, int64_t words, int32_t rows, int32_t* nmaps) {
+    const int64_t per_map = words * 4;
+    int64_t n = std::min<int64_t>(rows, h->sm_count);
+    n = std::min<int64_t>(n, std::max<int64_t>(1, kBitmapBudget / std::max<int64_t>(per_map, 1)));
+    n = std::max<int64_t>(n, 1);
+    const size_t need = static_cast<size_t>(n * per_map);
+    if (need > h->bitmap_bytes) {
+        if (h->bitmaps != nullptr) {
+            B200_TRY(cudaDeviceSynchronize());
+            B200_TRY(cudaFree(h->bitmaps));
+            h->bitmaps = nullptr;
+            h->bitmap_bytes = 0;
+        }
+        B200_TRY(cudaMalloc(reinterpret_cast<void**>(&h->bitmaps), need));
+        h->bitmap_bytes = need;
+    }
+    *nmaps = static_cast<int32_t>(n);
+    return SPGEMM_OK;
+}
+
+Ladder make_ladder(const BinLauncher* bins, int nb, int min_bin) {
+    Ladder l = {};
+    l.nb = nb;
+    l.min_bin = min_bin < 0 ? 0 : std::min(min_bin, nb - 1);
+    for (int i = 0; i < nb; i++) l.limit[i] = bins[i].limit;
+    return l;
+}
+
+spgemm_status fork_streams(spgemm_handle_s* h, cudaStream_t main) {
+    B200_TRY(cudaEventRecord(h->ev_fork, main));
+    for (int i = 0; i < h->nside; i++) B200_TRY(cudaStreamWaitEvent(h->side[i], h->ev_fork, 0));
+    return SPGEMM_OK;
+}
+
+spgemm_status join_streams(spgemm_handle_s* h, cudaStream_t main) {
+    for (int i = 0; i < h->nside; i++) {
+        B200_TRY(cudaEventRecord(h->ev_join[i], h->side[i]));
+        B200_TRY(cudaStreamWaitEvent(main, h->ev_join[i], 0));
+    }
+    return SPGEMM_OK;
+}
+
+spgemm_status check_view(const spgemm_csr_view* v, const char* name) {
+    if (v == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, std::string(name) + " is NULL");
+    if (v->m < 0 || v->n < 0 || v->nnz < 0)
+        return fail(SPGEMM_ERR_INVALID_ARG, std::string(name) + " has a negative dimension");
+    if (v->rpt == nullptr)
+        return fail(SPGEMM_ERR_INVALID_ARG, std::string(name) + ".rpt is NULL");
+    if (v->nnz > 0 && (v->col == nullptr || v->val == nullptr))
+        return fail(SPGEMM_ERR_INVALID_ARG, std::string(name) + ".col/.val is NULL");
+    return SPGEMM_OK;
+}
+
+spgemm_status status_to_error(const DevStatus& st) {
+    if (st.flags == 0u) return SPGEMM_OK;
+    char buf[256];
+    if (st.flags & kStBadInput) {
+        std::snprintf(buf, sizeof buf,
+                      "invalid operand: unsorted, duplicate or out-of-range column, or bad row "
+                      "pointer (row %d, check %d)",
+                      st.row, st.detail);
+        return fail(SPGEMM_ERR_INVALID_ARG, buf);
+    }
+    std::snprintf(buf, sizeof buf, "device status 0x%x at row %d (detail %d)", st.flags, st.row,
+                  st.detail);
+    return fail(SPGEMM_ERR_INTERNAL, buf);
+}
+
+spgemm_status sync_mirror(spgemm_handle_s* h, cudaStream_t stream, const Plan* plan,
+                          const Scratch& s) {
+    B200_TRY(cudaMemcpyAsync(&h->mirror->plan, plan, sizeof(Plan), cudaMemcpyDeviceToHost,
+                             stream));
+    B200_TRY(cudaMemcpyAsync(&h->mirror->status, s.status, sizeof(DevStatus),
+                             cudaMemcpyDeviceToHost, stream));
+    B200_TRY(cudaMemcpyAsync(&h->mirror->fail_count, s.fail_count, sizeof(int32_t),
+                             cudaMemcpyDeviceToHost, stream));
+    B200_TRY(cudaStreamSynchronize(stream));
+    h->info.host_syncs++;
+    return SPGEMM_OK;
+}
+
+cudaError_t prof_event(spgemm_handle_s* h, cudaEvent_t* ev) {
+    const size_t used = h->prof.size() * 2;
+    while (h->prof_events.size() < used + 2) {
+        cudaEvent_t e;
+        cudaError_t err = cudaEventCreate(&e);
+        if (err != cudaSuccess) return err;
+        h->prof_events.push_back(e);
+    }
+    ev[0] = h->prof_events[used];
+    ev[1] = h->prof_events[used + 1];
+    return cudaSuccess;
+}
+
+// Launch through `fn` on `stream`; with profiling on, bracket it by an event
+// pair recorded on the same stream.
+template<typename F>
+spgemm_status timed(spgemm_handle_s* h, const char* name, int phase, int bin, int rows,
+                    cudaStream_t stream, F&& fn) {
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    if (h->profile) {
+        B200_TRY(prof_event(h, ev));
+        B200_TRY(cudaEventRecord(ev[0], stream));
+    }
+    cudaError_t e = fn(stream);
+    if (e != cudaSuccess) return cuda_fail(e, name);
+    if (h->profile) {
+        B200_TRY(cudaEventRecord(ev[1], stream));
+        h->prof.push_back(ProfRec{name, phase, bin, rows, ev[0], ev[1]});
+    }
+    return SPGEMM_OK;
+}
+
+// After the stream is synchronised: turn the recorded pairs into durations.
+void resolve_profile(spgemm_handle_s* h) {
+    h->prof_done.clear();
+    for (const ProfRec& r : h->prof) {
+        spgemm_kernel_time k = {};
+        std::snprintf(k.name, sizeof k.name, "%s", r.name);
+        k.phase = r.phase;
+        k.bin = r.bin;
+        k.rows = r.rows;
+        float ms = -1.0f;
+        if (cudaEventElapsedTime(&ms, r.a, r.b) != cudaSuccess) ms = -1.0f;
+        k.ms = ms;
+        h->prof_done.push_back(k);
+    }
+    h->prof.clear();
+}
+
+// One kernel per non-empty bin, heavy bins first, round-robin over the side
+// streams (forked from and joined back into `main`).
+spgemm_status launch_bins(spgemm_handle_s* h, const BinLauncher* bins, int nb, int phase,
+                          const Plan& plan, const int32_t* row_lists, const ProductArgs& base,
+                          cudaStream_t main) {
+    if (spgemm_status st = fork_streams(h, main); st != SPGEMM_OK) return st;
+    int next = 0;
+    for (int b = nb - 1; b >= 0; b--) {
+        const int rows = plan.bin_size[b];
+        if (rows <= 0) continue;
+        ProductArgs a = base;
+        a.rows = row_lists + plan.bin_off[b];
+        a.nrows = rows;
+        cudaStream_t s = h->side[next % h->nside];
+        next++;
+        const BinLauncher& L = bins[b];
+        if (spgemm_status st = timed(h, L.name, phase, b, rows, s,
+                                     [&](cudaStream_t ss) { return L.launch(a, ss); });
+            st != SPGEMM_OK)
+            return st;
+    }
+    return join_streams(h, main);
+}
+
+template<typename V>
+spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm_csr_view* B,
+                      spgemm_csr_out* C, cudaStream_t stream) {
+    if (h == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "handle is NULL");
+    if (C == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "C is NULL");
+    if (spgemm_status st = check_view(A, "A"); st != SPGEMM_OK) return st;
+    if (spgemm_status st = check_view(B, "B"); st != SPGEMM_OK) return st;
+    if (A->n != B->m)
+        return fail(SPGEMM_ERR_INVALID_ARG, "A.n (" + std::to_string(A->n) +
+                                                ") must equal B.m (" + std::to_string(B->m) + ")");
+    std::memset(C, 0, sizeof(*C));
+    h->info = spgemm_info{};
+    h->prof.clear();
+    h->prof_done.clear();
+    B200_TRY(cudaSetDevice(h->device));
+
+    const int32_t m = A->m;
+    const int32_t n = B->n;
+    C->m = m;
+    C->n = n;
+
+    const BinLauncher* sym = nullptr;
+    const int nsym = sym1_ladder(&sym);
+    const BinLauncher* fil = nullptr;
+    const int nfil = sizeof(V) == 8 ? s2n_ladder_f64(&fil) : s2n_ladder_f32(&fil);
+    h->info.n_sym_bins = nsym;
+    h->info.n_num_bins = nfil;
+
+    int32_t* c_rpt = nullptr;
+    B200_TRY(cudaMallocAsync(reinterpret_cast<void**>(&c_rpt), sizeof(int32_t) * (size_t(m) + 1),
+                             stream));
+    C->rpt = c_rpt;
+    auto bail = [&](spgemm_status st) {
+        const std::string msg = g_last_error;
+        cudaStreamSynchronize(stream);
+        spgemm_csr_free(C, stream);
+        cudaStreamSynchronize(stream);
+        h->prof.clear();
+        g_last_error = msg;
+        return st;
+    };
+#define B200_STEP(expr)                                                  \
+    do {                                                                 \
+        spgemm_status st_ = (expr);                                      \
+        if (st_ != SPGEMM_OK) return bail(st_);                          \
+    } while (0)
+
+    Scratch s;
+    B200_STEP(ensure_scratch(h, m, &s));
+    // status, plans and fail counter are contiguous at the front of the scratch
+    if (cudaError_t e = cudaMemsetAsync(
+            h->scratch, 0, reinterpret_cast<char*>(s.hist1) - static_cast<char*>(h->scratch),
+            stream);
+        e != cudaSuccess)
+        return bail(cuda_fail(e, "memset scratch"));
+    if (h->checked) {
+        B200_STEP(timed(h, "check_csr_A", 0, -1, A->m, stream, [&](cudaStream_t ss) {
+            return launch_check_csr(A->rpt, A->col, A->m, A->n, A->nnz, s.status, ss);
+        }));
+        B200_STEP(timed(h, "check_csr_B", 0, -1, B->m, stream, [&](cudaStream_t ss) {
+            return launch_check_csr(B->rpt, B->col, B->m, B->n, B->nnz, s.status, ss);
+        }));
+        // no kernel indexes through an operand that failed validation
+        B200_STEP(sync_mirror(h, stream, s.plan1, s));
+        B200_STEP(status_to_error(h->mirror->status));
+    }
+    if (m == 0 || A->nnz == 0 || B->nnz == 0) {
+        if (cudaError_t e = cudaMemsetAsync(c_rpt, 0, sizeof(int32_t) * (size_t(m) + 1), stream);
+            e != cudaSuccess)
+            return bail(cuda_fail(e, "memset C.rpt"));
+        B200_STEP(sync_mirror(h, stream, s.plan1, s));
+        B200_STEP(status_to_error(h->mirror->status));
+        resolve_profile(h);
+        return SPGEMM_OK;
+    }
+
+    // ---- count pass: NIP per row and bins ---------------------------------
+    const int nctas = bin_ctas(m);
+    const Ladder lad1 = make_ladder(sym, nsym, h->min_sym_bin);
+    B200_STEP(timed(h, "nip_hist", 0, -1, m, stream, [&](cudaStream_t ss) {
+        return launch_nip_hist(A->rpt, A->col, B->rpt, m, c_rpt, s.hist1, s.plan1, s.status,
+                               lad1, ss);
+    }));
+    B200_STEP(timed(h, "bin_offsets", 0, -1, m, stream, [&](cudaStream_t ss) {
+        return launch_bin_offsets(s.hist1, nctas, nullptr, s.plan1, lad1, ss);
+    }));
+    B200_STEP(timed(h, "bin_scatter", 0, -1, m, stream, [&](cudaStream_t ss) {
+        return launch_bin_scatter(c_rpt, m, s.hist1, nullptr, s.bins1, s.plan1, lad1, false, ss);
+    }));
+    B200_STEP(sync_mirror(h, stream, s.plan1, s));
+    B200_STEP(status_to_error(h->mirror->status));
+    const Plan p1 = h->mirror->plan;
+    h->info.nip = p1.total_key;
+    h->info.max_row_nip = p1.max_key;
+    for (int b = 0; b < nsym && b < 16; b++) h->info.sym_bin_rows[b] = p1.bin_size[b];
+
+    ProductArgs pa = {};
+    pa.a_rpt = A->rpt;
+    pa.a_col = A->col;
+    pa.a_val = A->val;
+    pa.b_rpt = B->rpt;
+    pa.b_col = B->col;
+    pa.b_val = B->val;
+    pa.n_cols = n;
+    pa.c_rpt = c_rpt;
+    pa.status = s.status;
+    pa.cluster = h->cluster;
+    pa.fail_rows = s.fail_rows;
+    pa.fail_count = s.fail_count;
+    pa.words = (static_cast<int64_t>(n) + 31) / 32;
+
+    // ---- sym1: exact nnz per row --------------------------------------------
+    const int glob1 = nsym - 1;  // global bin (cluster spills, or the test knob)
+    const int clus1 = nsym - 2;  // cluster bin
+    const int32_t cluster_rows = p1.bin_size[clus1];
+    const int32_t global_rows = p1.bin_size[glob1];
+    if (cluster_rows > 0 || global_rows > 0) {
+        int32_t nmaps = 0;
+        B200_STEP(ensure_bitmaps(h, pa.words, std::max(cluster_rows, global_rows), &nmaps));
+        pa.bitmaps = h->bitmaps;
+        pa.nmaps = nmaps;
+    }
+    // cluster bin, then its spills, then knob-forced global rows: one chain on
+    // the first side stream; the other bins round-robin on the rest
+    B200_STEP(fork_streams(h, stream));
+    {
+        cudaStream_t chain = h->side[0];
+        if (cluster_rows > 0) {
+            ProductArgs a = pa;
+            a.rows = s.bins1 + p1.bin_off[clus1];
+            a.nrows = cluster_rows;
+            B200_STEP(timed(h, sym[clus1].name, 1, clus1, cluster_rows, chain,
+                            [&](cudaStream_t ss) { return sym[clus1].launch(a, ss); }));
+            // rows that spilled out of the cluster table: their count is only
+            // known on the device, so the global kernel runs on a grid of
+            // bitmap slots and reads its row count from the device
+            ProductArgs f = pa;
+            f.rows = s.fail_rows;
+            f.nrows = -1;
+            B200_STEP(timed(h, "sym1_global_spills", 1, glob1, -1, chain,
+                            [&](cudaStream_t ss) { return sym[glob1].launch(f, ss); }));
+        }
+        if (global_rows > 0) {
+            ProductArgs a = pa;
+            a.rows = s.bins1 + p1.bin_off[glob1];
+            a.nrows = global_rows;
+            B200_STEP(timed(h, sym[glob1].name, 1, glob1, global_rows, chain,
+                            [&](cudaStream_t ss) { return sym[glob1].launch(a, ss); }));
+        }
+        const bool chain_used = cluster_rows > 0 || global_rows > 0;
+        const int first = chain_used && h->nside > 1 ? 1 : 0;
+        int next = first;
+        for (int b = clus1 - 1; b >= 0; b--) {
+            const int rows = p1.bin_size[b];
+            if (rows <= 0) continue;
+            ProductArgs a = pa;
+            a.rows = s.bins1 + p1.bin_off[b];
+            a.nrows = rows;
+            B200_STEP(timed(h, sym[b].name, 1, b, rows, h->side[next],
+                            [&](cudaStream_t ss) { return sym[b].launch(a, ss); }));
+            next = next + 1 < h->nside ? next + 1 : first;
+        }
+    }
+    B200_STEP(join_streams(h, stream));
+
+    // ---- scan pass: row pointer and fill bins -------------------------------
+    const Ladder lad2 = make_ladder(fil, nfil, h->min_num_bin);
+    B200_STEP(timed(h, "nnz_hist", 2, -1, m, stream, [&](cudaStream_t ss) {
+        return launch_nnz_hist(c_rpt, m, s.hist2, s.cta_sum, s.plan2, lad2, ss);
+    }));
+    B200_STEP(timed(h, "scan_offsets", 2, -1, m, stream, [&](cudaStream_t ss) {
+        return launch_bin_offsets(s.hist2, nctas, s.cta_sum, s.plan2, lad2, ss);
+    }));
+    B200_STEP(timed(h, "scan_scatter", 2, -1, m, stream, [&](cudaStream_t ss) {
+        return launch_bin_scatter(c_rpt, m, s.hist2, s.cta_sum, s.bins2, s.plan2, lad2, true,
+                                  ss);
+    }));
+    B200_STEP(sync_mirror(h, stream, s.plan2, s));
+    B200_STEP(status_to_error(h->mirror->status));
+    const Plan p2 = h->mirror->plan;
+    h->info.sym_fail_rows = h->mirror->fail_count;
+    if (p2.overflow)
+        return bail(fail(SPGEMM_ERR_OVERFLOW,
+                         "nnz(C) = " + std::to_string(p2.total_key) + " exceeds int32"));
+    const int32_t nnz = static_cast<int32_t>(p2.total_key);
+    h->info.nnz = nnz;
+    h->info.max_row_nnz = p2.max_key;
+    for (int b = 0; b < nfil && b < 16; b++) h->info.num_bin_rows[b] = p2.bin_size[b];
+    C->nnz = nnz;
+    if (nnz == 0) {
+        resolve_profile(h);
+        return SPGEMM_OK;
+    }
+
+    // ---- fill + sort + numeric ----------------------------------------------
+    // C.col gets 16 bytes of tail padding so 16-byte-granular staging of a
+    // row's tail never leaves the allocation
+    if (cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&C->col),
+                                        sizeof(int32_t) * size_t(nnz) + 16, stream);
+        e != cudaSuccess)
+        return bail(cuda_fail(e, "allocate C.col"));
+    if (cudaError_t e = cudaMallocAsync(&C->val, sizeof(V) * size_t(nnz), stream);
+        e != cudaSuccess)
+        return bail(cuda_fail(e, "allocate C.val"));
+    pa.c_col = C->col;
+    pa.c_val = C->val;
+    if (p2.bin_size[nfil - 1] > 0) {
+        int32_t nmaps = 0;
+        B200_STEP(ensure_bitmaps(h, pa.words, p2.bin_size[nfil - 1], &nmaps));
+        pa.bitmaps = h->bitmaps;
+        pa.nmaps = nmaps;
+    }
+    B200_STEP(launch_bins(h, fil, nfil, 3, p2, s.bins2, pa, stream));
+    if (cudaError_t e = cudaMemcpyAsync(&h->mirror->status, s.status, sizeof(DevStatus),
+                                        cudaMemcpyDeviceToHost, stream);
+        e != cudaSuccess)
+        return bail(cuda_fail(e, "read status"));
+    if (cudaError_t e = cudaStreamSynchronize(stream); e != cudaSuccess)
+        return bail(cuda_fail(e, "final synchronize"));
+    h->info.host_syncs++;
+    B200_STEP(status_to_error(h->mirror->status));
+    resolve_profile(h);
+#undef B200_STEP
+    return SPGEMM_OK;
+}
+
+template<typename V>
+spgemm_status product_host(spgemm_handle_s* h, const spgemm_csr_view* A,
+                           const spgemm_csr_view* B, spgemm_csr_out* C, cudaStream_t stream) {
+    if (h == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "handle is NULL");
+    if (C == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "C is NULL");
+    if (spgemm_status st = check_view(A, "A"); st != SPGEMM_OK) return st;
+    if (spgemm_status st = check_view(B, "B"); st != SPGEMM_OK) return st;
+    B200_TRY(cudaSetDevice(h->device));
+    auto bytes_of = [](const spgemm_csr_view* v) {
+        return align_up(sizeof(int32_t) * (size_t(v->m) + 1), 256) +
+               align_up(sizeof(int32_t) * size_t(v->nnz), 256) +
+               align_up(sizeof(V) * size_t(v->nnz), 256);
+    };
+    const size_t need = bytes_of(A) + bytes_of(B);
+    if (need > h->in_bytes) {
+        if (h->in_buf != nullptr) {
+            B200_TRY(cudaDeviceSynchronize());
+            B200_TRY(cudaFree(h->in_buf));
+            h->in_buf = nullptr;
+            h->in_bytes = 0;
+        }
+        B200_TRY(cudaMalloc(&h->in_buf, need));
+        h->in_bytes = need;
+    }
+    char* p = static_cast<char*>(h->in_buf);
+    auto upload = [&](const spgemm_csr_view* v, spgemm_csr_view* d) -> cudaError_t {
+        *d = *v;
+        int32_t* rpt = reinterpret_cast<int32_t*>(p);
+        p += align_up(sizeof(int32_t) * (size_t(v->m) + 1), 256);
+        int32_t* col = reinterpret_cast<int32_t*>(p);
+        p += align_up(sizeof(int32_t) * size_t(v->nnz), 256);
+        V* val = reinterpret_cast<V*>(p);
+        p += align_up(sizeof(V) * size_t(v->nnz), 256);
+        cudaError_t e = cudaMemcpyAsync(rpt, v->rpt, sizeof(int32_t) * (size_t(v->m) + 1),
+                                        cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess && v->nnz > 0)
+            e = cudaMemcpyAsync(col, v->col, sizeof(int32_t) * size_t(v->nnz),
+                                cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess && v->nnz > 0)
+            e = cudaMemcpyAsync(val, v->val, sizeof(V) * size_t(v->nnz), cudaMemcpyHostToDevice,
+                                stream);
+        d->rpt = rpt;
+        d->col = col;
+        d->val = val;
+        return e;
+    };
+    spgemm_csr_view dA, dB;
+    B200_TRY(upload(A, &dA));
+    B200_TRY(upload(B, &dB));
+    spgemm_csr_out dC;
+    if (spgemm_status st = product<V>(h, &dA, &dB, &dC, stream); st != SPGEMM_OK) return st;
+    std::memset(C, 0, sizeof(*C));
+    C->m = dC.m;
+    C->n = dC.n;
+    C->nnz = dC.nnz;
+    C->rpt = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * (size_t(dC.m) + 1)));
+    C->col = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * std::max<size_t>(dC.nnz, 1)));
+    C->val = std::malloc(sizeof(V) * std::max<size_t>(dC.nnz, 1));
+    if (C->rpt == nullptr || C->col == nullptr || C->val == nullptr) {
+        spgemm_host_csr_free(C);
+        spgemm_csr_free(&dC, stream);
+        return fail(SPGEMM_ERR_OOM, "host allocation of C failed");
+    }
+    cudaError_t e = cudaMemcpyAsync(C->rpt, dC.rpt, sizeof(int32_t) * (size_t(dC.m) + 1),
+                                    cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess && dC.nnz > 0)
+        e = cudaMemcpyAsync(C->col, dC.col, sizeof(int32_t) * size_t(dC.nnz),
+                            cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess && dC.nnz > 0)
+        e = cudaMemcpyAsync(C->val, dC.val, sizeof(V) * size_t(dC.nnz), cudaMemcpyDeviceToHost,
+                            stream);
+    spgemm_csr_free(&dC, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        spgemm_host_csr_free(C);
+        return cuda_fail(e, "copy C to host");
+    }
+    return SPGEMM_OK;
+}
+
+}  // namespace
+}  // namespace b200
+
+using namespace b200;
+
+extern "C" {
+
+int spgemm_abi_version(void) { return SPGEMM_ABI_VERSION; }
+
+const char* spgemm_last_error_string(void) { return g_last_error.c_str(); }
+
+const char* spgemm_status_string(spgemm_status st) {
+    switch (st) {
+        case SPGEMM_OK: return "SPGEMM_OK";
+        case SPGEMM_ERR_INVALID_ARG: return "SPGEMM_ERR_INVALID_ARG";
+        case SPGEMM_ERR_OOM: return "SPGEMM_ERR_OOM";
+        case SPGEMM_ERR_UNSUPPORTED_DEVICE: return "SPGEMM_ERR_UNSUPPORTED_DEVICE";
+        case SPGEMM_ERR_OVERFLOW: return "SPGEMM_ERR_OVERFLOW";
+        case SPGEMM_ERR_TIMEOUT: return "SPGEMM_ERR_TIMEOUT";
+        case SPGEMM_ERR_CUDA: return "SPGEMM_ERR_CUDA";
+        case SPGEMM_ERR_INTERNAL: return "SPGEMM_ERR_INTERNAL";
+    }
+    return "SPGEMM_ERR_UNKNOWN";
+}
+
+spgemm_status spgemm_create(spgemm_handle_t* handle, int device) {
+    if (handle == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "handle is NULL");
+    *handle = nullptr;
+    int dev = device;
+    if (dev < 0) B200_TRY(cudaGetDevice(&dev));
+    int major = 0;
+    int minor = 0;
+    B200_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    B200_TRY(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev));
+    if (major != 10 || minor != 0)
+        return fail(SPGEMM_ERR_UNSUPPORTED_DEVICE,
+                    "compute capability " + std::to_string(major) + "." + std::to_string(minor) +
+                        " is not sm_100 (this library is built for sm_100a only)");
+    B200_TRY(cudaSetDevice(dev));
+    auto* h = new spgemm_handle_s();
+    h->device = dev;
+    B200_TRY(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, dev));
+    B200_TRY(sym1_prepare());
+    B200_TRY(s2n_prepare());
+    for (int i = 0; i < kMaxSide; i++) {
+        B200_TRY(cudaStreamCreateWithFlags(&h->side[i], cudaStreamNonBlocking));
+        B200_TRY(cudaEventCreateWithFlags(&h->ev_join[i], cudaEventDisableTiming));
+    }
+    B200_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+    B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&h->mirror), sizeof(HostMirror)));
+    *handle = h;
+    return SPGEMM_OK;
+}
+
+spgemm_status spgemm_destroy(spgemm_handle_t h) {
+    if (h == nullptr) return SPGEMM_OK;
+    cudaSetDevice(h->device);
+    cudaDeviceSynchronize();
+    for (int i = 0; i < kMaxSide; i++) {
+        if (h->side[i]) cudaStreamDestroy(h->side[i]);
+        if (h->ev_join[i]) cudaEventDestroy(h->ev_join[i]);
+    }
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->scratch) cudaFree(h->scratch);
+    if (h->bitmaps) cudaFree(h->bitmaps);
+    if (h->in_buf) cudaFree(h->in_buf);
+    if (h->mirror) cudaFreeHost(h->mirror);
+    for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
+    delete h;
+    return SPGEMM_OK;
+}
+
+spgemm_status spgemm_csr_f64(spgemm_handle_t h, const spgemm_csr_view* A,
+                             const spgemm_csr_view* B, spgemm_csr_out* C, void* stream) {
+    return product<double>(h, A, B, C, static_cast<cudaStream_t>(stream));
+}
+
+spgemm_status spgemm_csr_f32(spgemm_handle_t h, const spgemm_csr_view* A,
+                             const spgemm_csr_view* B, spgemm_csr_out* C, void* stream) {
+    return product<float>(h, A, B, C, static_cast<cudaStream_t>(stream));
+}
+
+spgemm_status spgemm_csr_host_f64(spgemm_handle_t h, const spgemm_csr_view* A,
+                                  const spgemm_csr_view* B, spgemm_csr_out* C, void* stream) {
+    return product_host<double>(h, A, B, C, static_cast<cudaStream_t>(stream));
+}
+
+spgemm_status spgemm_csr_host_f32(spgemm_handle_t h, const spgemm_csr_view* A,
+                                  const spgemm_csr_view* B, spgemm_csr_out* C, void* stream) {
+    return product_host<float>(h, A, B, C, static_cast<cudaStream_t>(stream));
+}
+
+spgemm_status spgemm_csr_free(spgemm_csr_out* C, void* stream) {
+    if (C == nullptr) return SPGEMM_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaSuccess;
+    if (C->rpt) e = cudaFreeAsync(C->rpt, s);
+    if (C->col && e == cudaSuccess) e = cudaFreeAsync(C->col, s);
+    if (C->val && e == cudaSuccess) e = cudaFreeAsync(C->val, s);
+    std::memset(C, 0, sizeof(*C));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFreeAsync");
+    return SPGEMM_OK;
+}
+
+spgemm_status spgemm_host_csr_free(spgemm_csr_out* C) {
+    if (C == nullptr) return SPGEMM_OK;
+    std::free(C->rpt);
+    std::free(C->col);
+    std::free(C->val);
+    std::memset(C, 0, sizeof(*C));
+    return SPGEMM_OK;
+}
+
+spgemm_status spgemm_get_nip(spgemm_handle_t h, const spgemm_csr_view* A,
+                             const spgemm_csr_view* B, int64_t* nip, void* stream) {
+    if (h == nullptr || nip == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "NULL argument");
+    if (spgemm_status st = check_view(A, "A"); st != SPGEMM_OK) return st;
+    if (spgemm_status st = check_view(B, "B"); st != SPGEMM_OK) return st;
+    if (A->n != B->m) return fail(SPGEMM_ERR_INVALID_ARG, "A.n must equal B.m");
+    B200_TRY(cudaSetDevice(h->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Scratch sc;
+    if (spgemm_status st = ensure_scratch(h, A->m, &sc); st != SPGEMM_OK) return st;
+    long long* d = reinterpret_cast<long long*>(sc.cta_sum);
+    B200_TRY(cudaMemsetAsync(d, 0, sizeof(long long), s));
+    B200_TRY(launch_total_nip(A->rpt, A->col, B->rpt, A->m, d, s));
+    long long v = 0;
+    B200_TRY(cudaMemcpyAsync(&h->mirror->plan.total_key, d, sizeof(long long),
+                             cudaMemcpyDeviceToHost, s));
+    B200_TRY(cudaStreamSynchronize(s));
+    v = h->mirror->plan.total_key;
+    *nip = v;
+    return SPGEMM_OK;
+}
+
+spgemm_status spgemm_last_profile(spgemm_handle_t h, spgemm_kernel_time* out, int32_t capacity,
+                                  int32_t* count) {
+    if (h == nullptr || count == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "NULL argument");
+    const int32_t n = static_cast<int32_t>(h->prof_done.size());
+    *count = n;
+    if (out != nullptr)
+        for (int32_t i = 0; i < n && i < capacity; i++) out[i] = h->prof_done[i];
+    return SPGEMM_OK;
+}
+
+spgemm_status spgemm_last_info(spgemm_handle_t h, spgemm_info* info) {
+    if (h == nullptr || info == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "NULL argument");
+    *info = h->info;
+    return SPGEMM_OK;
+}
+
+spgemm_status spgemm_set_option(spgemm_handle_t h, spgemm_option opt, int64_t value) {
+    if (h == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "handle is NULL");
+    switch (opt) {
+        case SPGEMM_OPT_CHECKED: h->checked = value != 0; return SPGEMM_OK;
+        case SPGEMM_OPT_MIN_SYM_BIN: h->min_sym_bin = static_cast<int>(value); return SPGEMM_OK;
+        case SPGEMM_OPT_MIN_NUM_BIN: h->min_num_bin = static_cast<int>(value); return SPGEMM_OK;
+        case SPGEMM_OPT_CLUSTER_SIZE:
+            if (value != 2 && value != 4 && value != 8)
+                return fail(SPGEMM_ERR_INVALID_ARG, "cluster size must be 2, 4 or 8");
+            h->cluster = static_cast<int>(value);
+            return SPGEMM_OK;
+        case SPGEMM_OPT_STREAMS:
+            if (value < 1 || value > kMaxSide)
+                return fail(SPGEMM_ERR_INVALID_ARG, "streams must be in 1..8");
+            h->nside = static_cast<int>(value);
+            return SPGEMM_OK;
+        case SPGEMM_OPT_PROFILE: h->profile = value != 0; return SPGEMM_OK;
+    }
+    return fail(SPGEMM_ERR_INVALID_ARG, "unknown option");
+}
+
+spgemm_status spgemm_get_option(spgemm_handle_t h, spgemm_option opt, int64_t* value) {
+    if (h == nullptr || value == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "NULL argument");
+    switch (opt) {
+        case SPGEMM_OPT_CHECKED: *value = h->checked; return SPGEMM_OK;
+        case SPGEMM_OPT_MIN_SYM_BIN: *value = h->min_sym_bin; return SPGEMM_OK;
+        case SPGEMM_OPT_MIN_NUM_BIN: *value = h->min_num_bin; return SPGEMM_OK;
+        case SPGEMM_OPT_CLUSTER_SIZE: *value = h->cluster; return SPGEMM_OK;
+        case SPGEMM_OPT_STREAMS: *value = h->nside; return SPGEMM_OK;
+        case SPGEMM_OPT_PROFILE: *value = h->profile; return SPGEMM_OK;
+    }
+    return fail(SPGEMM_ERR_INVALID_ARG, "unknown option");
+}
+
+spgemm_status spgemm_ladder_info(spgemm_handle_t h, int which, int dtype_bytes, int* n_bins,
+                                 int64_t* limits) {
+    (void)h;
+    if (n_bins == nullptr || limits == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "NULL");
+    const BinLauncher* l = nullptr;
+    int nb = 0;
+    if (which == 0) {
+        nb = sym1_ladder(&l);
+    } else {
+        nb = dtype_bytes == 8 ? s2n_ladder_f64(&l) : s2n_ladder_f32(&l);
+    }
+    *n_bins = nb;
+    for (int i = 0; i < 16; i++) limits[i] = i < nb ? l[i].limit : 0;
+    return SPGEMM_OK;
+}
+
+}  // extern "C"

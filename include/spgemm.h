@@ -1,0 +1,200 @@
+/*
+ * spgemm.h -- C ABI of the B200 (sm_100a) CSR SpGEMM library, libspgemm_b200.so.
+ *
+ * This is the drop-in boundary for the reference's hot path
+ *     template<std::floating_point T>
+ *     utils::DeviceCSR<T> proposal::proposal(const utils::DeviceCSR<T>& A,
+ *                                            const utils::DeviceCSR<T>& B);
+ * (geektrove/GPUSpGEMM src/libproposal/include/proposal/proposal.cuh:85-124),
+ * which has no C ABI of its own.  Every entry point below names the reference
+ * interface it replaces.  A header-only C++ shim with the reference's exact
+ * signature sits in gpuspgemm_b200/csrc/b200_proposal.hpp.
+ *
+ * Conventions (same as the reference's utils::CSR, csr.cuh:22-31):
+ *   - CSR with 0-based int32 indices: rpt[m+1], col[nnz], val[nnz];
+ *   - columns of B sorted ascending and duplicate-free within each row
+ *     (the binary-search numeric relies on it, num.cuh:104-116);
+ *   - T is float or double (two entry points per operation).
+ * Output C: m = A.m, n = B.n, sorted duplicate-free columns, every structural
+ * product kept (an entry whose value cancels to 0.0 stays in C).
+ *
+ * Streams are passed as `void*` holding a cudaStream_t (NULL = legacy default
+ * stream).  All device pointers are plain CUDA device addresses.
+ */
+#ifndef SPGEMM_B200_H
+#define SPGEMM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPGEMM_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define SPGEMM_API __attribute__((visibility("default")))
+#else
+#define SPGEMM_API
+#endif
+
+/* Error codes.  The reference throws std::runtime_error from
+ * utils::handle_cuda_error (src/libutils/include/utils/errors.cuh:11-22) and on
+ * an unsupported device (proposal.cuh:123); the C ABI returns these instead and
+ * spgemm_last_error_string() carries the message. */
+typedef enum spgemm_status {
+    SPGEMM_OK = 0,
+    SPGEMM_ERR_INVALID_ARG = 1,        /* NULL pointer, negative size, A.n != B.m,
+                                          unsorted/duplicate/out-of-range columns
+                                          (checked mode) */
+    SPGEMM_ERR_OOM = 2,                /* device or pinned-host allocation failed */
+    SPGEMM_ERR_UNSUPPORTED_DEVICE = 3, /* not an sm_100 device */
+    SPGEMM_ERR_OVERFLOW = 4,           /* nnz(C) does not fit int32 */
+    SPGEMM_ERR_TIMEOUT = 5,            /* a bounded device wait ran out */
+    SPGEMM_ERR_CUDA = 6,               /* a CUDA runtime call failed */
+    SPGEMM_ERR_INTERNAL = 7            /* a kernel reported a bounded-probe or
+                                          capacity failure through its status word */
+} spgemm_status;
+
+typedef struct spgemm_handle_s* spgemm_handle_t;
+
+/* Read-only CSR operand.  Replaces const utils::DeviceCSR<T>& (csr.cuh:22-31). */
+typedef struct spgemm_csr_view {
+    int32_t m;
+    int32_t n;
+    int32_t nnz;
+    const int32_t* rpt;
+    const int32_t* col;
+    const void* val; /* float* or double* to match the entry point */
+} spgemm_csr_view;
+
+/* CSR result.  Replaces the owning utils::DeviceCSR<T> that proposal() returns.
+ * Device results are allocated by the library with cudaMallocAsync on the call's
+ * stream, exactly like the reference (setup.cuh:146, binning.cuh:236,
+ * sym2.cuh:396), so cudaFree() releases them as ~CSR does (csr.cuh:241-252);
+ * spgemm_csr_free() does the same stream-ordered. */
+typedef struct spgemm_csr_out {
+    int32_t m;
+    int32_t n;
+    int32_t nnz;
+    int32_t* rpt;
+    int32_t* col;
+    void* val;
+} spgemm_csr_out;
+
+/* Statistics of the most recent product on a handle. */
+typedef struct spgemm_info {
+    int64_t nip;             /* intermediate products = FLOP / 2 (nip.cuh:52-78) */
+    int64_t nnz;             /* nnz(C) */
+    int32_t max_row_nip;     /* max NIP over rows of C (setup.cuh:29-95) */
+    int32_t max_row_nnz;     /* max nnz over rows of C (binning.cuh:213-217) */
+    int32_t sym_bin_rows[16]; /* rows per symbolic-count bin */
+    int32_t num_bin_rows[16]; /* rows per fill+numeric bin */
+    int32_t sym_fail_rows;   /* rows whose cluster table overflowed -> global bin */
+    int32_t n_sym_bins;
+    int32_t n_num_bins;
+    int32_t host_syncs;      /* host round-trips taken by the call */
+} spgemm_info;
+
+/* ---- lifecycle ------------------------------------------------------------ */
+
+/* Create a handle bound to CUDA device `device` (-1 = current device).  The
+ * handle owns scratch memory, side streams and pinned staging, reused across
+ * calls (the reference creates MAX_N_BINS streams and its scratch per call,
+ * setup.cuh:164-165, cleanup.cuh:15-31).  One handle per host thread. */
+SPGEMM_API spgemm_status spgemm_create(spgemm_handle_t* handle, int device);
+SPGEMM_API spgemm_status spgemm_destroy(spgemm_handle_t handle);
+
+/* ---- the product ---------------------------------------------------------- */
+
+/* C = A * B on the device.  Replaces proposal::proposal<double> / <float>
+ * (proposal.cuh:85-124) and its phases setup / binning / sym1 / sym_binning2 /
+ * sym2 / num / cleanup (setup.cuh:134-178, binning.cuh:146-243,
+ * sym1.cuh:311-463, sym2.cuh:293-404, num.cuh:303-442, cleanup.cuh:15-31).
+ * A, B: device arrays.  C: filled with library-allocated device arrays.
+ * Synchronous on return, like the reference (cleanup.cuh:30). */
+SPGEMM_API spgemm_status spgemm_csr_f64(spgemm_handle_t handle, const spgemm_csr_view* A,
+                             const spgemm_csr_view* B, spgemm_csr_out* C, void* stream);
+SPGEMM_API spgemm_status spgemm_csr_f32(spgemm_handle_t handle, const spgemm_csr_view* A,
+                             const spgemm_csr_view* B, spgemm_csr_out* C, void* stream);
+
+/* Release a device result (stream-ordered cudaFreeAsync); replaces ~CSR for
+ * Location::Device (csr.cuh:114-117, runtime.cuh:59-66).  Zeroes *C. */
+SPGEMM_API spgemm_status spgemm_csr_free(spgemm_csr_out* C, void* stream);
+
+/* C = A * B with HOST operands and a HOST result: copies A and B to the device,
+ * multiplies, copies C back.  Replaces the apps' convert/run pair
+ * (src/apps/proposal.cu:15-26: HostCSR::to<Device>, proposal, to<Host>).
+ * C's arrays are malloc()'d host memory; release with spgemm_host_csr_free. */
+SPGEMM_API spgemm_status spgemm_csr_host_f64(spgemm_handle_t handle, const spgemm_csr_view* A,
+                                  const spgemm_csr_view* B, spgemm_csr_out* C,
+                                  void* stream);
+SPGEMM_API spgemm_status spgemm_csr_host_f32(spgemm_handle_t handle, const spgemm_csr_view* A,
+                                  const spgemm_csr_view* B, spgemm_csr_out* C,
+                                  void* stream);
+SPGEMM_API spgemm_status spgemm_host_csr_free(spgemm_csr_out* C);
+
+/* Total intermediate products of A*B (FLOP = 2 * nip).  Replaces
+ * utils::get_nip (src/libutils/include/utils/nip.cuh:52-78). */
+SPGEMM_API spgemm_status spgemm_get_nip(spgemm_handle_t handle, const spgemm_csr_view* A,
+                             const spgemm_csr_view* B, int64_t* nip, void* stream);
+
+/* Statistics of the last product run on `handle`. */
+SPGEMM_API spgemm_status spgemm_last_info(spgemm_handle_t handle, spgemm_info* info);
+
+/* ---- options -------------------------------------------------------------- */
+
+typedef enum spgemm_option {
+    /* Validate operands on the device before multiplying (sorted, duplicate-free,
+     * in-range columns; monotone rpt).  0 = off (default), 1 = on. */
+    SPGEMM_OPT_CHECKED = 1,
+    /* Test knob: every non-empty row goes to at least this bin of the symbolic
+     * count ladder (-1 = off).  Exercises each kernel variant on small inputs,
+     * like the reference's per-bin parameter tables (parameters.cuh:29-153). */
+    SPGEMM_OPT_MIN_SYM_BIN = 2,
+    /* Test knob: same for the fill + numeric ladder (-1 = off). */
+    SPGEMM_OPT_MIN_NUM_BIN = 3,
+    /* Cluster size (CTAs) of the distributed-shared-memory bins: 2, 4 or 8. */
+    SPGEMM_OPT_CLUSTER_SIZE = 4,
+    /* Number of side streams the bins are spread over (1..8). */
+    SPGEMM_OPT_STREAMS = 5,
+    /* Record a CUDA event pair around every kernel launch of a product; read
+     * the durations with spgemm_last_profile.  0 = off (default), 1 = on. */
+    SPGEMM_OPT_PROFILE = 6
+} spgemm_option;
+
+SPGEMM_API spgemm_status spgemm_set_option(spgemm_handle_t handle, spgemm_option option, int64_t value);
+SPGEMM_API spgemm_status spgemm_get_option(spgemm_handle_t handle, spgemm_option option, int64_t* value);
+
+/* Per-launch device time of the last product (SPGEMM_OPT_PROFILE on), timed
+ * with CUDA events on the stream each kernel was launched on.  The reference
+ * marks the same phases with NVTX ranges (proposal.cuh:30, setup.cuh:139,
+ * sym1.cuh:316, sym2.cuh:298, num.cuh:308). */
+typedef struct spgemm_kernel_time {
+    char name[48];  /* kernel variant, e.g. "s2n_team8_t64" */
+    int32_t phase;  /* 0 count binning, 1 count, 2 scan binning, 3 fill+numeric */
+    int32_t bin;    /* ladder bin, -1 for binning kernels */
+    int32_t rows;   /* rows the launch handled (-1 if only known on the device) */
+    float ms;       /* event-timed duration */
+} spgemm_kernel_time;
+
+SPGEMM_API spgemm_status spgemm_last_profile(spgemm_handle_t handle, spgemm_kernel_time* out,
+                                             int32_t capacity, int32_t* count);
+
+/* Number of bins of each ladder and the key limit of bin `bin` (rows whose
+ * key -- NIP for the count ladder, nnz for the fill ladder -- is <= limit). */
+SPGEMM_API spgemm_status spgemm_ladder_info(spgemm_handle_t handle, int which /*0 sym, 1 num*/,
+                                 int dtype_bytes, int* n_bins, int64_t* limits /*[16]*/);
+
+/* ---- errors / version ----------------------------------------------------- */
+
+/* Message of the last error raised on the calling thread ("" if none). */
+SPGEMM_API const char* spgemm_last_error_string(void);
+SPGEMM_API const char* spgemm_status_string(spgemm_status status);
+SPGEMM_API int spgemm_abi_version(void);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* SPGEMM_B200_H */

@@ -1,0 +1,220 @@
+"""GPU parity: the sm_100a library against the CPU oracle (and the reference's
+own GPU build where it is present), through the C ABI.
+
+Bar: row pointers and sorted column indices bit-exact; values within
+    FP64: 1e-12 relative per entry,   FP32 (accumulated in FP32): 1e-5,
+stated as (a) max |dc|/|c_ref| over entries with c_ref != 0 -- asserted where
+the inputs cannot cancel (all values positive) -- and (b) the cancellation-
+aware max |dc| / sum_k |a_ik||b_kj|, asserted everywhere.
+"""
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from gpuspgemm_b200 import generators as G
+from gpuspgemm_b200.csr import HostCSR, load_csr
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+TOL = {np.dtype(np.float64): 1e-12, np.dtype(np.float32): 1e-5}
+RESULTS = []
+
+
+def gpu_product(A: HostCSR, B: HostCSR, handle, dtype) -> HostCSR:
+    from gpuspgemm_b200.api import DeviceCSR, proposal
+    dA = DeviceCSR.from_host(A.astype(dtype))
+    dB = DeviceCSR.from_host(B.astype(dtype))
+    return proposal(dA, dB, handle).to_host()
+
+
+def check(oracle, A, B, C, dtype, name, positive=False):
+    dtype = np.dtype(dtype)
+    A64 = A.astype(dtype).astype(np.float64)  # the rounded inputs, exactly
+    B64 = B.astype(dtype).astype(np.float64)
+    R = oracle.spgemm(A64, B64, np.float64)
+    res = oracle.compare(C, R, oracle.abs_bound(A64, B64, R))
+    res["case"] = name
+    res["dtype"] = dtype.name
+    RESULTS.append(res)
+    assert res["rpt_equal"], res
+    assert res["col_equal"], res
+    assert res.get("max_cond", 0.0) <= TOL[dtype], res
+    if positive:
+        assert res["max_rel"] <= TOL[dtype], res
+    return res
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _dump_results():
+    yield
+    out = Path(os.environ.get("SPGEMM_PARITY_OUT", "gpurun_out"))
+    if out.is_dir():
+        (out / "parity_results.json").write_text(json.dumps(RESULTS, indent=1, default=str))
+
+
+def test_uniform_4096x8_f64(handle, oracle_mod):
+    A = G.uniform_rows(4096, 8)
+    C = gpu_product(A, A, handle, np.float64)
+    check(oracle_mod, A, A, C, np.float64, "uniform4096x8")
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_power_law_small(handle, oracle_mod, dtype):
+    A = G.power_law(30000, 2.0, 3000, seed=21)
+    C = gpu_product(A, A, handle, dtype)
+    check(oracle_mod, A, A, C, dtype, "powerlaw30000", positive=True)
+
+
+def test_power_law_1m_f64(handle, oracle_mod):
+    """Full-size power-law C = A*A (n = 1e6, Zipf 2.0, cap 4700)."""
+    A = G.power_law()
+    C = gpu_product(A, A, handle, np.float64)
+    check(oracle_mod, A, A, C, np.float64, "powerlaw1M", positive=True)
+
+
+def test_rectangular(handle, oracle_mod):
+    A = G.uniform_rows(700, 9, seed=31, m=500)
+    B = G.uniform_rows(300, 7, seed=32, m=700)
+    C = gpu_product(A, B, handle, np.float64)
+    assert (C.m, C.n) == (500, 300)
+    check(oracle_mod, A, B, C, np.float64, "rect500x700x300")
+
+
+def _ladder_len(handle, which):
+    return len(handle.ladder(which, 8))
+
+
+@pytest.mark.parametrize("b", range(9))
+def test_forced_sym_bin(handle, oracle_mod, b):
+    """Every row routed to at least count bin b: each kernel variant runs."""
+    from gpuspgemm_b200 import _native as N
+    if b >= _ladder_len(handle, 0):
+        pytest.skip("no such bin")
+    A = G.power_law(3000, 2.0, 300, seed=41)
+    handle.set_option(N.OPT_MIN_SYM_BIN, b)
+    try:
+        C = gpu_product(A, A, handle, np.float64)
+    finally:
+        handle.set_option(N.OPT_MIN_SYM_BIN, -1)
+    check(oracle_mod, A, A, C, np.float64, f"forced_sym_bin{b}", positive=True)
+
+
+@pytest.mark.parametrize("b", range(9))
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_forced_num_bin(handle, oracle_mod, b, dtype):
+    from gpuspgemm_b200 import _native as N
+    if b >= _ladder_len(handle, 1):
+        pytest.skip("no such bin")
+    A = G.power_law(3000, 2.0, 300, seed=42)
+    handle.set_option(N.OPT_MIN_NUM_BIN, b)
+    try:
+        C = gpu_product(A, A, handle, dtype)
+    finally:
+        handle.set_option(N.OPT_MIN_NUM_BIN, -1)
+    check(oracle_mod, A, A, C, dtype, f"forced_num_bin{b}", positive=True)
+
+
+def test_heavy_row_spills_to_global(handle, oracle_mod):
+    """One row with ~190k distinct columns: past the cluster table, so the
+    count spills to the global bitmap and the fill runs in the global bin."""
+    rng = np.random.default_rng(51)
+    B = G.uniform_rows(300_000, 300, seed=52, m=1000)
+    a_col = np.arange(1000, dtype=np.int32)
+    A = HostCSR(3, 1000, np.array([0, 1000, 1000, 1003], np.int32),
+                np.concatenate([a_col, np.array([1, 5, 9], np.int32)]),
+                rng.uniform(0.1, 1.0, 1003))
+    C = gpu_product(A, B, handle, np.float64)
+    info = handle.info()
+    check(oracle_mod, A, B, C, np.float64, "heavy_row_spill", positive=False)
+    assert info["max_row_nnz"] > 150_000
+
+
+def test_edge_cases(handle, oracle_mod):
+    # empty rows in A, empty rows in B, rows of A that hit only empty B rows
+    A = HostCSR(6, 5, np.array([0, 0, 2, 2, 3, 5, 5], np.int32),
+                np.array([0, 3, 4, 1, 2], np.int32), np.array([2.0, -1.0, 1.5, 1.0, 3.0]))
+    B = HostCSR(5, 4, np.array([0, 2, 2, 2, 4, 5], np.int32),
+                np.array([1, 3, 0, 1, 2], np.int32), np.array([1.0, 2.0, 4.0, -2.0, 0.5]))
+    C = gpu_product(A, B, handle, np.float64)
+    check(oracle_mod, A, B, C, np.float64, "empty_rows")
+    # cancellation to an exact zero keeps the entry
+    A = HostCSR(2, 2, np.array([0, 2, 2], np.int32), np.array([0, 1], np.int32),
+                np.array([1.0, 1.0]))
+    B = HostCSR(2, 1, np.array([0, 1, 2], np.int32), np.array([0, 0], np.int32),
+                np.array([1.0, -1.0]))
+    C = gpu_product(A, B, handle, np.float64)
+    assert C.nnz == 1 and C.val.tolist() == [0.0]
+
+
+def test_empty_operands(handle):
+    A = HostCSR(4, 3, np.zeros(5, np.int32), np.zeros(0, np.int32), np.zeros(0))
+    B = G.uniform_rows(5, 2, seed=1, m=3)
+    C = gpu_product(A, B, handle, np.float64)
+    assert (C.m, C.n, C.nnz) == (4, 5) + (0,) and np.all(C.rpt == 0)
+    Z = HostCSR(0, 3, np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0))
+    C = gpu_product(Z, B, handle, np.float64)
+    assert (C.m, C.nnz) == (0, 0)
+
+
+def test_dimension_mismatch_raises(handle):
+    from gpuspgemm_b200 import SpgemmError
+    A = G.uniform_rows(10, 2, seed=1, m=5)
+    B = G.uniform_rows(10, 2, seed=2, m=11)
+    with pytest.raises(SpgemmError, match="INVALID_ARG"):
+        gpu_product(A, B, handle, np.float64)
+
+
+def test_checked_mode_rejects_unsorted(handle):
+    from gpuspgemm_b200 import SpgemmError
+    from gpuspgemm_b200 import _native as N
+    A = G.uniform_rows(50, 4, seed=3)
+    bad = HostCSR(A.m, A.n, A.rpt.copy(), A.col.copy(), A.val.copy())
+    bad.col[0], bad.col[1] = bad.col[1], bad.col[0]
+    handle.set_option(N.OPT_CHECKED, 1)
+    try:
+        with pytest.raises(SpgemmError, match="INVALID_ARG"):
+            gpu_product(A, bad, handle, np.float64)
+        C = gpu_product(A, A, handle, np.float64)  # valid input still works
+        assert C.nnz > 0
+    finally:
+        handle.set_option(N.OPT_CHECKED, 0)
+
+
+def test_host_entry_point_and_nip(handle, oracle_mod):
+    from gpuspgemm_b200.api import DeviceCSR, get_nip, proposal_host
+    A = G.power_law(5000, 2.0, 500, seed=61)
+    C = proposal_host(A, A, handle)
+    check(oracle_mod, A, A, C, np.float64, "host_entry", positive=True)
+    dA = DeviceCSR.from_host(A)
+    assert get_nip(dA, dA, handle) == oracle_mod.nip(A, A)
+    assert handle.info()["nip"] == oracle_mod.nip(A, A)
+
+
+def test_repeat_calls_same_structure(handle):
+    A = G.power_law(20000, 2.0, 1000, seed=71)
+    C1 = gpu_product(A, A, handle, np.float64)
+    C2 = gpu_product(A, A, handle, np.float64)
+    assert np.array_equal(C1.rpt, C2.rpt) and np.array_equal(C1.col, C2.col)
+    assert np.allclose(C1.val, C2.val, rtol=1e-13, atol=0)
+
+
+def _golden():
+    man = GOLDEN / "manifest.json"
+    return sorted(json.loads(man.read_text()).items()) if man.exists() else []
+
+
+@pytest.mark.parametrize("name,entry", _golden() or [pytest.param(
+    None, None, marks=pytest.mark.skip(reason="golden vectors not generated"))])
+def test_against_reference_golden(handle, oracle_mod, name, entry):
+    """The library against the reference's own outputs on the same inputs."""
+    dt = np.dtype(entry["dtype"])
+    A = load_csr(GOLDEN / f"{name}.A.csr", dt)
+    B = load_csr(GOLDEN / f"{name}.B.csr", dt)
+    C = gpu_product(A, B, handle, dt)
+    R = load_csr(GOLDEN / f"{name}.C_proposal.csr", dt)
+    assert np.array_equal(C.rpt, R.rpt) and np.array_equal(C.col, R.col)
+    check(oracle_mod, A, B, C, dt, f"golden_{name}")
