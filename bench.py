@@ -278,12 +278,13 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
         del Ch
-    e2e_total = float(sum(e2e_ms))
+    e2e_total = float(sum(e2e_ms)) if e2e_ms else float("nan")
     if world > 1:
         t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
-    e2e_value = 2.0 * nip * args.e2e_steps * world / (e2e_total / 1e3) / 1e9
+    e2e_value = (2.0 * nip * args.e2e_steps * world / (e2e_total / 1e3) / 1e9
+                 if e2e_ms else None)
 
     if rank != 0:
         h.close()
@@ -356,13 +357,15 @@ def run_ours(args, rank, world, local_rank):
         "dtype": args.dtype, "data": "synthetic (seeded generator)",
         "config": config_of(args, A, nip, nnz_c),
         "e2e": {"value": e2e_value, "unit": "GFLOPS", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_total / args.e2e_steps},
+                "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_total / args.e2e_steps if e2e_ms else None},
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": launches,
         "kernels": kernels[:12],
         "host_syncs_per_step": info["host_syncs"],
+        "host_phase_us_last_step": h.info()["phase_us"],
     }
     h.close()
     return line

@@ -64,6 +64,7 @@ class Info(C.Structure):
         ("n_sym_bins", C.c_int32),
         ("n_num_bins", C.c_int32),
         ("host_syncs", C.c_int32),
+        ("phase_us", C.c_float * 8),
     ]
 
 

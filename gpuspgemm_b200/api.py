@@ -79,6 +79,7 @@ class Handle:
             "num_bin_rows": list(inf.num_bin_rows)[: inf.n_num_bins],
             "sym_fail_rows": int(inf.sym_fail_rows),
             "host_syncs": int(inf.host_syncs),
+            "phase_us": [round(float(x), 1) for x in inf.phase_us][:7],
         }
 
     def profile(self) -> list[dict]:
@@ -230,10 +231,35 @@ def _host_view(a: HostCSR) -> tuple[N.CsrView, list]:
     return v, keep
 
 
+class _HostResultOwner:
+    """Returns a host result's page-locked block to the library pool
+    (spgemm_host_csr_free) once no array refers to it."""
+
+    def __init__(self, out: N.CsrOut):
+        self.out = out
+
+    def __del__(self):
+        try:
+            N.lib().spgemm_host_csr_free(C.byref(self.out))
+        except Exception:
+            pass
+
+
+class _HostLibraryArray:
+    """Library-owned host memory exposed through __array_interface__; the numpy
+    array built from it keeps it (and so the owner) alive."""
+
+    def __init__(self, owner, ptr: int, n: int, typestr: str):
+        self._owner = owner
+        self.__array_interface__ = {"shape": (n,), "typestr": typestr,
+                                    "data": (ptr, False), "version": 3}
+
+
 def proposal_host(A: HostCSR, B: HostCSR, handle: Handle | None = None,
                   stream=None) -> HostCSR:
     """C = A * B from host operands to a host result through the C ABI's host
-    entry point (copies inside the call, like the apps' convert/run/to<Host>)."""
+    entry point (copies inside the call, like the apps' convert/run/to<Host>).
+    The result arrays are zero-copy views of the library's page-locked block."""
     if A.val.dtype != B.val.dtype:
         raise TypeError("A and B must have the same value dtype")
     h = handle or default_handle()
@@ -244,20 +270,12 @@ def proposal_host(A: HostCSR, B: HostCSR, handle: Handle | None = None,
     fn = N.lib().spgemm_csr_host_f64 if f64 else N.lib().spgemm_csr_host_f32
     sp = _stream_ptr(stream) if torch is not None and torch.cuda.is_available() else None
     N.check(fn(h.ptr, C.byref(va), C.byref(vb), C.byref(out), sp))
-    m, n = int(out.m), int(out.n)
-    try:
-        vdt = np.float64 if f64 else np.float32
-        rpt = np.ctypeslib.as_array(C.cast(out.rpt, C.POINTER(C.c_int32)), (out.m + 1,)).copy()
-        if out.nnz > 0:
-            col = np.ctypeslib.as_array(C.cast(out.col, C.POINTER(C.c_int32)), (out.nnz,)).copy()
-            cval = C.cast(out.val, C.POINTER(C.c_double if f64 else C.c_float))
-            val = np.ctypeslib.as_array(cval, (out.nnz,)).astype(vdt, copy=True)
-        else:
-            col = np.zeros(0, np.int32)
-            val = np.zeros(0, vdt)
-    finally:
-        N.lib().spgemm_host_csr_free(C.byref(out))
     del ka, kb
+    owner = _HostResultOwner(out)
+    m, n, nnz = int(out.m), int(out.n), int(out.nnz)
+    rpt = np.asarray(_HostLibraryArray(owner, out.rpt, m + 1, "<i4"))
+    col = np.asarray(_HostLibraryArray(owner, out.col, nnz, "<i4"))
+    val = np.asarray(_HostLibraryArray(owner, out.val, nnz, "<f8" if f64 else "<f4"))
     return HostCSR(m, n, rpt, col, val)
 
 

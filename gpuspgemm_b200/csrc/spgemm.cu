@@ -14,9 +14,11 @@
 // creates/destroys its streams and scratch in every call (setup.cuh:164-165,
 // cleanup.cuh:15-31); here streams, events and scratch live in the handle.
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -104,6 +106,10 @@ struct spgemm_handle_s {
     int min_num_bin = -1;
     int cluster = 4;
     int profile = 0;
+    // C's arrays come from this stream-ordered pool; it keeps freed memory
+    // mapped (release threshold = max) so repeated products do not re-map
+    // hundreds of MB per call.  cudaFree / cudaFreeAsync release them.
+    cudaMemPool_t pool = nullptr;
     spgemm_info info = {};
     // profiling: an event pair per launch, resolved after the final sync
     std::vector<b200::ProfRec> prof;
@@ -343,8 +349,14 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     h->info.n_num_bins = nfil;
 
     int32_t* c_rpt = nullptr;
-    B200_TRY(cudaMallocAsync(reinterpret_cast<void**>(&c_rpt), sizeof(int32_t) * (size_t(m) + 1),
-                             stream));
+    const auto t_start = std::chrono::steady_clock::now();
+    auto mark = [&](int i) {
+        h->info.phase_us[i] = static_cast<float>(
+            std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t_start)
+                .count());
+    };
+    B200_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&c_rpt),
+                                     sizeof(int32_t) * (size_t(m) + 1), h->pool, stream));
     C->rpt = c_rpt;
     auto bail = [&](spgemm_status st) {
         const std::string msg = g_last_error;
@@ -403,7 +415,9 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     B200_STEP(timed(h, "bin_scatter", 0, -1, m, stream, [&](cudaStream_t ss) {
         return launch_bin_scatter(c_rpt, m, s.hist1, nullptr, s.bins1, s.plan1, lad1, false, ss);
     }));
+    mark(0);
     B200_STEP(sync_mirror(h, stream, s.plan1, s));
+    mark(1);
     B200_STEP(status_to_error(h->mirror->status));
     const Plan p1 = h->mirror->plan;
     h->info.nip = p1.total_key;
@@ -491,7 +505,9 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         return launch_bin_scatter(c_rpt, m, s.hist2, s.cta_sum, s.bins2, s.plan2, lad2, true,
                                   ss);
     }));
+    mark(2);
     B200_STEP(sync_mirror(h, stream, s.plan2, s));
+    mark(3);
     B200_STEP(status_to_error(h->mirror->status));
     const Plan p2 = h->mirror->plan;
     h->info.sym_fail_rows = h->mirror->fail_count;
@@ -511,11 +527,12 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     // ---- fill + sort + numeric ----------------------------------------------
     // C.col gets 16 bytes of tail padding so 16-byte-granular staging of a
     // row's tail never leaves the allocation
-    if (cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&C->col),
-                                        sizeof(int32_t) * size_t(nnz) + 16, stream);
+    if (cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&C->col),
+                                                sizeof(int32_t) * size_t(nnz) + 16, h->pool,
+                                                stream);
         e != cudaSuccess)
         return bail(cuda_fail(e, "allocate C.col"));
-    if (cudaError_t e = cudaMallocAsync(&C->val, sizeof(V) * size_t(nnz), stream);
+    if (cudaError_t e = cudaMallocFromPoolAsync(&C->val, sizeof(V) * size_t(nnz), h->pool, stream);
         e != cudaSuccess)
         return bail(cuda_fail(e, "allocate C.val"));
     pa.c_col = C->col;
@@ -526,18 +543,59 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         pa.bitmaps = h->bitmaps;
         pa.nmaps = nmaps;
     }
+    mark(4);
     B200_STEP(launch_bins(h, fil, nfil, 3, p2, s.bins2, pa, stream));
+    mark(5);
     if (cudaError_t e = cudaMemcpyAsync(&h->mirror->status, s.status, sizeof(DevStatus),
                                         cudaMemcpyDeviceToHost, stream);
         e != cudaSuccess)
         return bail(cuda_fail(e, "read status"));
     if (cudaError_t e = cudaStreamSynchronize(stream); e != cudaSuccess)
         return bail(cuda_fail(e, "final synchronize"));
+    mark(6);
     h->info.host_syncs++;
     B200_STEP(status_to_error(h->mirror->status));
     resolve_profile(h);
 #undef B200_STEP
     return SPGEMM_OK;
+}
+
+// Page-locked host blocks for host results, reused across calls (process
+// wide, so spgemm_host_csr_free needs no handle).  A result's three arrays
+// share one block; freeing the result returns the block to the pool.
+struct PinnedBlock {
+    void* p;
+    size_t bytes;
+    bool used;
+};
+std::mutex g_pin_mu;
+std::vector<PinnedBlock> g_pin;
+
+void* pinned_take(size_t bytes) {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    PinnedBlock* best = nullptr;
+    for (PinnedBlock& b : g_pin)
+        if (!b.used && b.bytes >= bytes && (best == nullptr || b.bytes < best->bytes)) best = &b;
+    if (best != nullptr) {
+        best->used = true;
+        return best->p;
+    }
+    const size_t rounded = align_up(bytes + bytes / 8, size_t(2) << 20);
+    void* p = nullptr;
+    if (cudaMallocHost(&p, rounded) != cudaSuccess) return nullptr;
+    g_pin.push_back(PinnedBlock{p, rounded, true});
+    return p;
+}
+
+bool pinned_give_back(void* p) {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    for (PinnedBlock& b : g_pin) {
+        if (b.p == p) {
+            b.used = false;
+            return true;
+        }
+    }
+    return false;
 }
 
 template<typename V>
@@ -595,14 +653,18 @@ spgemm_status product_host(spgemm_handle_s* h, const spgemm_csr_view* A,
     C->m = dC.m;
     C->n = dC.n;
     C->nnz = dC.nnz;
-    C->rpt = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * (size_t(dC.m) + 1)));
-    C->col = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * std::max<size_t>(dC.nnz, 1)));
-    C->val = std::malloc(sizeof(V) * std::max<size_t>(dC.nnz, 1));
-    if (C->rpt == nullptr || C->col == nullptr || C->val == nullptr) {
-        spgemm_host_csr_free(C);
+    const size_t rpt_b = align_up(sizeof(int32_t) * (size_t(dC.m) + 1), 256);
+    const size_t col_b = align_up(sizeof(int32_t) * std::max<size_t>(dC.nnz, 1), 256);
+    const size_t val_b = align_up(sizeof(V) * std::max<size_t>(dC.nnz, 1), 256);
+    char* blk = static_cast<char*>(pinned_take(rpt_b + col_b + val_b));
+    if (blk == nullptr) {
+        std::memset(C, 0, sizeof(*C));
         spgemm_csr_free(&dC, stream);
-        return fail(SPGEMM_ERR_OOM, "host allocation of C failed");
+        return fail(SPGEMM_ERR_OOM, "page-locked host allocation of C failed");
     }
+    C->rpt = reinterpret_cast<int32_t*>(blk);
+    C->col = reinterpret_cast<int32_t*>(blk + rpt_b);
+    C->val = blk + rpt_b + col_b;
     cudaError_t e = cudaMemcpyAsync(C->rpt, dC.rpt, sizeof(int32_t) * (size_t(dC.m) + 1),
                                     cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess && dC.nnz > 0)
@@ -670,6 +732,13 @@ spgemm_status spgemm_create(spgemm_handle_t* handle, int device) {
     }
     B200_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&h->mirror), sizeof(HostMirror)));
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    B200_TRY(cudaMemPoolCreate(&h->pool, &props));
+    uint64_t keep = UINT64_MAX;
+    B200_TRY(cudaMemPoolSetAttribute(h->pool, cudaMemPoolAttrReleaseThreshold, &keep));
     *handle = h;
     return SPGEMM_OK;
 }
@@ -688,6 +757,8 @@ spgemm_status spgemm_destroy(spgemm_handle_t h) {
     if (h->in_buf) cudaFree(h->in_buf);
     if (h->mirror) cudaFreeHost(h->mirror);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
+    // outstanding results keep the pool alive until they are freed
+    if (h->pool) cudaMemPoolDestroy(h->pool);
     delete h;
     return SPGEMM_OK;
 }
@@ -726,9 +797,11 @@ spgemm_status spgemm_csr_free(spgemm_csr_out* C, void* stream) {
 
 spgemm_status spgemm_host_csr_free(spgemm_csr_out* C) {
     if (C == nullptr) return SPGEMM_OK;
-    std::free(C->rpt);
-    std::free(C->col);
-    std::free(C->val);
+    if (C->rpt != nullptr && !pinned_give_back(C->rpt)) {
+        std::free(C->rpt);
+        std::free(C->col);
+        std::free(C->val);
+    }
     std::memset(C, 0, sizeof(*C));
     return SPGEMM_OK;
 }

@@ -69,9 +69,10 @@ typedef struct spgemm_csr_view {
 } spgemm_csr_view;
 
 /* CSR result.  Replaces the owning utils::DeviceCSR<T> that proposal() returns.
- * Device results are allocated by the library with cudaMallocAsync on the call's
- * stream, exactly like the reference (setup.cuh:146, binning.cuh:236,
- * sym2.cuh:396), so cudaFree() releases them as ~CSR does (csr.cuh:241-252);
+ * Device results are stream-ordered allocations on the call's stream, as in the
+ * reference (cudaMallocAsync, setup.cuh:146, binning.cuh:236, sym2.cuh:396),
+ * taken from the handle's memory pool (which keeps freed memory mapped), so
+ * cudaFree() releases them as ~CSR does (csr.cuh:241-252);
  * spgemm_csr_free() does the same stream-ordered. */
 typedef struct spgemm_csr_out {
     int32_t m;
@@ -94,6 +95,10 @@ typedef struct spgemm_info {
     int32_t n_sym_bins;
     int32_t n_num_bins;
     int32_t host_syncs;      /* host round-trips taken by the call */
+    /* host-side microseconds since the call began, at: count binning queued,
+     * host sync 1 done, count kernels queued, host sync 2 done, C allocated,
+     * fill kernels queued, final sync done (unused entries 0) */
+    float phase_us[8];
 } spgemm_info;
 
 /* ---- lifecycle ------------------------------------------------------------ */
@@ -125,7 +130,9 @@ SPGEMM_API spgemm_status spgemm_csr_free(spgemm_csr_out* C, void* stream);
 /* C = A * B with HOST operands and a HOST result: copies A and B to the device,
  * multiplies, copies C back.  Replaces the apps' convert/run pair
  * (src/apps/proposal.cu:15-26: HostCSR::to<Device>, proposal, to<Host>).
- * C's arrays are malloc()'d host memory; release with spgemm_host_csr_free. */
+ * C's three arrays live in one page-locked block from a process-wide pool
+ * (so the device-to-host copy runs at full link speed); spgemm_host_csr_free
+ * returns the block to the pool. */
 SPGEMM_API spgemm_status spgemm_csr_host_f64(spgemm_handle_t handle, const spgemm_csr_view* A,
                                   const spgemm_csr_view* B, spgemm_csr_out* C,
                                   void* stream);
