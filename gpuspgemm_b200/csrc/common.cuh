@@ -28,7 +28,8 @@ enum : unsigned {
     kStCapacity = 2u,     // a row did not fit the bin it was routed to
     kStBadInput = 4u,     // checked mode found an invalid operand
     kStNipOverflow = 8u,  // a row's NIP does not fit int32
-    kStClusterFail = 16u  // (diagnostic) a cluster row spilled to the global bin
+    kStClusterFail = 16u, // (diagnostic) a cluster row spilled to the global bin
+    kStIndex = 32u        // a computed shared-memory index or alignment failed its check
 };
 
 struct DevStatus {

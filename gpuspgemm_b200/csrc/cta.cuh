@@ -13,7 +13,7 @@ struct CtaScratch {
     int32_t bs[THREADS];   // B-row start of each A entry of the chunk
     int32_t warp_tot[THREADS / kWarp];
     int32_t total;
-    int32_t pad[3];
+    int32_t aux[3];  // per-row words of the kernels (e.g. the fill's Dmax)
 };
 
 // Inclusive scan of one int per thread over the CTA.  Contains two

@@ -1,0 +1,89 @@
+"""GPU: the library against the REFERENCE's own GPU code on the same inputs.
+
+oracle/_ref/libref_proposal.so is the reference's proposal_inner<T,
+Parameters<CC80>> and its cuSPARSE-ALG2 validate path, compiled from the
+reference sources for sm_100a (`make -C oracle ref`).  These tests need that
+build; they are skipped where it is absent.  Besides parity they time both
+implementations the way the reference's `measure` lambda does (wall clock
+around the call plus a device synchronize, C allocated and freed inside;
+src/apps/proposal.cu:28-35) and write the figures to
+gpurun_out/ref_compare.json.
+"""
+import json
+import os
+import time
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from gpuspgemm_b200 import generators as G
+
+pytestmark = pytest.mark.gpu
+
+OUT = Path(os.environ.get("SPGEMM_PARITY_OUT", "gpurun_out"))
+RECORDS = {}
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _dump():
+    yield
+    if OUT.is_dir() and RECORDS:
+        (OUT / "ref_compare.json").write_text(json.dumps(RECORDS, indent=1))
+
+
+def _ours_times(A, dtype, handle, warmups=3, runs=5):
+    import torch
+
+    from gpuspgemm_b200.api import DeviceCSR, proposal
+    dA = DeviceCSR.from_host(A.astype(dtype))
+    for _ in range(warmups):
+        C = proposal(dA, dA, handle)
+        del C
+    ts = []
+    for _ in range(runs):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        C = proposal(dA, dA, handle)
+        del C
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    C = proposal(dA, dA, handle).to_host()
+    return ts, C
+
+
+CASES = {
+    "uniform4096x8_f64": (lambda: G.uniform_rows(4096, 8), np.float64),
+    "powerlaw1M_f64": (lambda: G.power_law(), np.float64),
+    "powerlaw1M_f32": (lambda: G.power_law(), np.float32),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_against_reference_build(handle, oracle_mod, name):
+    if not oracle_mod.ref_available():
+        pytest.skip("oracle/_ref not built")
+    make, dt = CASES[name]
+    A = make().astype(dt)
+    R = oracle_mod.ref_proposal(A, A, dt)
+    ts, C = _ours_times(A, dt, handle)
+    assert np.array_equal(C.rpt, R.rpt), "row pointers differ from the reference"
+    assert np.array_equal(C.col, R.col), "column indices differ from the reference"
+    rel = np.abs(C.val.astype(np.float64) - R.val.astype(np.float64))
+    denom = np.abs(R.val.astype(np.float64))
+    nz = denom > 0
+    max_rel = float((rel[nz] / denom[nz]).max()) if np.any(nz) else 0.0
+    tol = 1e-12 if dt == np.float64 else 1e-5
+    assert max_rel <= tol, max_rel
+    ref_ts, nip = oracle_mod.ref_time("proposal", A, A, dt, warmups=3, runs=5)
+    rec = {"nip": nip, "nnz_C": int(C.nnz), "max_rel_vs_reference": max_rel,
+           "ours_s": ts, "reference_proposal_s": ref_ts,
+           "ours_gflops_median": 2 * nip / float(np.median(ts)) / 1e9,
+           "reference_gflops_median": 2 * nip / float(np.median(ref_ts)) / 1e9}
+    try:
+        cs_ts, _ = oracle_mod.ref_time("cusparse2", A, A, dt, warmups=1, runs=3)
+        rec["cusparse2_s"] = cs_ts
+        rec["cusparse2_gflops_median"] = 2 * nip / float(np.median(cs_ts)) / 1e9
+    except Exception as e:  # the reference records failed cuSPARSE runs as 0
+        rec["cusparse2_error"] = str(e)
+    RECORDS[name] = rec
