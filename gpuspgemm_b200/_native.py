@@ -101,6 +101,8 @@ SIGNATURES = {
     "spgemm_get_option": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]),
     "spgemm_ladder_info": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int),
                                      C.POINTER(C.c_int64)]),
+    "spgemm_row_nnz_noalloc": (C.c_int, [C.POINTER(CsrView), C.POINTER(CsrView), C.c_void_p,
+                                         C.c_void_p]),
     "spgemm_last_error_string": (C.c_char_p, []),
     "spgemm_status_string": (C.c_char_p, [C.c_int]),
     "spgemm_abi_version": (C.c_int, []),

@@ -683,6 +683,9 @@ spgemm_status product_host(spgemm_handle_s* h, const spgemm_csr_view* A,
 }
 
 }  // namespace
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
 }  // namespace b200
 
 using namespace b200;

@@ -193,6 +193,36 @@ SPGEMM_API spgemm_status spgemm_last_profile(spgemm_handle_t handle, spgemm_kern
 SPGEMM_API spgemm_status spgemm_ladder_info(spgemm_handle_t handle, int which /*0 sym, 1 num*/,
                                  int dtype_bytes, int* n_bins, int64_t* limits /*[16]*/);
 
+/* ---- allocation-free row sizes --------------------------------------------- */
+
+/* Largest B.n that spgemm_row_nnz_noalloc accepts. */
+#define SPGEMM_NOALLOC_MAX_COLS (1 << 20)
+
+/* Exact number of nonzeros of every row of C = A * B, written to the caller's
+ * device array c_row_nnz[A.m], WITHOUT allocating anything: no cudaMalloc,
+ * cudaMallocAsync, cudaFree or allocating library call, and no handle (a
+ * handle owns allocated scratch).  No counterpart in the reference: it is for
+ * callers that cannot allocate at the point where they size a product, for
+ * example because all device memory is already owned by their own pool, or
+ * because an allocation there would synchronise the device.  The caller can
+ * scan the counts into a row pointer and allocate C from its own memory.
+ *
+ * Only the index arrays of A and B are read (val may be NULL).  B's columns
+ * must lie in [0, B.n) with B.n <= SPGEMM_NOALLOC_MAX_COLS; larger B.n is
+ * rejected with SPGEMM_ERR_INVALID_ARG.  Runs on the current device and
+ * returns without synchronising (stream-ordered on `stream`).
+ *
+ * Scratch: a fixed 4 MiB bitmap area compiled into the library's device image
+ * (every GPU that loads the library holds it until the process exits).  The
+ * first call on a device looks up that area's device address
+ * (cudaGetSymbolAddress), so make the first call on each device outside any
+ * stream capture.  Every call uses the same area and clears it first, so calls
+ * that overlap on the GPU (other streams, other host threads) race: serialise
+ * them. */
+SPGEMM_API spgemm_status spgemm_row_nnz_noalloc(const spgemm_csr_view* A,
+                                                const spgemm_csr_view* B, int32_t* c_row_nnz,
+                                                void* stream);
+
 /* ---- errors / version ----------------------------------------------------- */
 
 /* Message of the last error raised on the calling thread ("" if none). */
