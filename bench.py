@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--out", type=str, default="")
+    ap.add_argument("--mode", choices=["plain", "batch"], default="plain",
+                    help="plain: the headline C=A*A workload; batch: many independent "
+                         "products (batched form vs one call per product)")
+    ap.add_argument("--batch-count", type=int, default=4096)
     return ap.parse_args()
 
 
@@ -103,6 +107,27 @@ def bin_rows(keys, limits, min_bin=0):
     b = np.searchsorted(np.asarray(limits, dtype=np.int64), keys, side="left")
     b = np.maximum(b, min_bin)
     return b
+
+
+# ---- multi-rank aggregation --------------------------------------------------
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """Max of a per-rank figure over all ranks (the timed region's duration):
+    an all-reduce MAX through the default process group (NCCL on GPUs, gloo in
+    the CPU tests).  Every rank must call it, in the same order."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_gflops(nip: int, steps: int, world: int, max_ms: float) -> float:
+    """Whole-job GFLOPS of N replicas: every rank multiplied the workload
+    `steps` times; the job took the slowest rank's time."""
+    return 2.0 * nip * steps * world / (max_ms / 1e3) / 1e9
 
 
 # ---- clocks -----------------------------------------------------------------
@@ -249,14 +274,10 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(float(sum(step_ms)), world, dev)
     h.set_option(N.OPT_PROFILE, 0)
 
-    value = 2.0 * nip * args.steps * world / (total_ms / 1e3) / 1e9
+    value = replica_gflops(nip, args.steps, world, total_ms)
 
     # e2e through the host-buffer entry point, pinned inputs
     pin = {k: torch.from_numpy(np.ascontiguousarray(getattr(A, k))).pin_memory()
@@ -278,13 +299,8 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
         del Ch
-    e2e_total = float(sum(e2e_ms)) if e2e_ms else float("nan")
-    if world > 1:
-        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = (2.0 * nip * args.e2e_steps * world / (e2e_total / 1e3) / 1e9
-                 if e2e_ms else None)
+    e2e_total = max_over_ranks(float(sum(e2e_ms)) if e2e_ms else float("nan"), world, dev)
+    e2e_value = replica_gflops(nip, args.e2e_steps, world, e2e_total) if e2e_ms else None
 
     if rank != 0:
         h.close()
@@ -371,12 +387,77 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+# ---- batched form: thousands of independent products --------------------------
+
+def run_batch(args, local_rank):
+    import torch
+
+    from gpuspgemm_b200 import generators as G
+    from gpuspgemm_b200.api import DeviceCSR, Handle, PackedBatch, batch, proposal
+
+    torch.cuda.set_device(local_rank)
+    dt = torch.float32 if args.dtype == "f32" else torch.float64
+    a_off, b_off, c_off, A, B = G.batch_packed_gpu(args.batch_count, seed=args.seed, dtype=dt)
+    pb = PackedBatch(a_off, b_off, c_off, A, B)
+    h = Handle(local_rank)
+    out = None
+    for _ in range(max(args.warmup, 1)):
+        out = batch(pb, h)
+        del out
+    info = h.info()
+    nip, nnz_c, groups = info["nip"], info["nnz"], h._last_groups
+    stream = torch.cuda.current_stream()
+    ts = []
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out = batch(pb, h)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+            del out
+    batch_ms = float(np.mean(ts))
+    # the same products as one plain call each (row-range view of the packed A)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(pb.count):
+        r0, r1 = int(a_off[i]), int(a_off[i + 1])
+        Ai = DeviceCSR(r1 - r0, A.n, A.rpt[r0:r1 + 1], A.col, A.val)
+        Ci = proposal(Ai, B, h)
+        del Ci
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    h.close()
+    return {
+        "metric": "batched independent products: products/s (and GFLOPS = 2*NIP/s)",
+        "value": pb.count / (batch_ms / 1e3), "unit": "products/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": batch_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": args.dtype, "data": "synthetic (seeded, generated on the device)",
+        "config": {"workload": f"{pb.count} independent square products, rows log-uniform "
+                               "[64, 16384], nnz/row ~ Poisson(U[6, 40]), uniform columns",
+                   "rows_total": int(a_off[-1]), "nnz_A": A.nnz, "nnz_B": B.nnz,
+                   "nip": nip, "nnz_C": nnz_c, "groups": groups},
+        "gflops": 2.0 * nip / (batch_ms / 1e3) / 1e9,
+        "plain_calls": {"ms_total": plain_ms, "products_per_s": pb.count / (plain_ms / 1e3),
+                        "gflops": 2.0 * nip / (plain_ms / 1e3) / 1e9},
+        "speedup_vs_plain_calls": plain_ms / batch_ms,
+        "clocks": clk.summary(),
+    }
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
+    if args.mode == "batch":
+        line = run_batch(args, local_rank) if rank == 0 else None
+    elif args.impl == "reference":
         line = run_reference(args, rank)
     else:
         if world > 1:

@@ -78,6 +78,25 @@ class KernelTime(C.Structure):
     ]
 
 
+class BatchDesc(C.Structure):
+    _fields_ = [
+        ("count", C.c_int32),
+        ("a_row_off", C.c_void_p),
+        ("b_row_off", C.c_void_p),
+        ("c_col_off", C.c_void_p),
+    ]
+
+
+class BatchOut(C.Structure):
+    _fields_ = [
+        ("count", C.c_int32),
+        ("products", C.POINTER(CsrOut)),
+        ("n_blocks", C.c_int32),
+        ("blocks", C.POINTER(C.c_void_p)),
+        ("n_groups", C.c_int32),
+    ]
+
+
 # name -> (restype, argtypes); must list every function spgemm.h declares
 SIGNATURES = {
     "spgemm_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int]),
@@ -101,6 +120,11 @@ SIGNATURES = {
     "spgemm_get_option": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]),
     "spgemm_ladder_info": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int),
                                      C.POINTER(C.c_int64)]),
+    "spgemm_batch_f64": (C.c_int, [C.c_void_p, C.POINTER(BatchDesc), C.POINTER(CsrView),
+                                   C.POINTER(CsrView), C.POINTER(BatchOut), C.c_void_p]),
+    "spgemm_batch_f32": (C.c_int, [C.c_void_p, C.POINTER(BatchDesc), C.POINTER(CsrView),
+                                   C.POINTER(CsrView), C.POINTER(BatchOut), C.c_void_p]),
+    "spgemm_batch_free": (C.c_int, [C.POINTER(BatchOut), C.c_void_p]),
     "spgemm_row_nnz_noalloc": (C.c_int, [C.POINTER(CsrView), C.POINTER(CsrView), C.c_void_p,
                                          C.c_void_p]),
     "spgemm_last_error_string": (C.c_char_p, []),

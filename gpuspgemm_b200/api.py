@@ -222,6 +222,101 @@ def _wrap_result(out: N.CsrOut, dtype) -> DeviceCSR:
     return DeviceCSR(out.m, out.n, rpt, col, val)
 
 
+class _BatchOwner:
+    """Frees a batch result (spgemm_batch_free) once no product view refers to it."""
+
+    def __init__(self, out: N.BatchOut):
+        self.out = out
+
+    def __del__(self):
+        try:
+            N.lib().spgemm_batch_free(C.byref(self.out), None)
+        except Exception:
+            pass
+
+
+@dataclass
+class PackedBatch:
+    """A batch of independent products C_i = A_i * B_i as block-diagonal CSR
+    operands (global column indices) plus host offset arrays."""
+
+    a_row_off: np.ndarray  # int32 [count + 1]
+    b_row_off: np.ndarray  # int32 [count + 1]
+    c_col_off: np.ndarray  # int32 [count + 1]
+    A: DeviceCSR
+    B: DeviceCSR
+
+    @property
+    def count(self) -> int:
+        return int(self.a_row_off.shape[0] - 1)
+
+
+def pack_batch(pairs) -> PackedBatch:
+    """Pack [(A_i, B_i)] (DeviceCSR, A_i.n == B_i.m) into block-diagonal operands."""
+    _require_torch()
+    As = [a for a, _ in pairs]
+    Bs = [b for _, b in pairs]
+    for a, b in pairs:
+        if a.n != b.m:
+            raise ValueError("A_i.n must equal B_i.m")
+        if a.dtype != As[0].dtype or b.dtype != As[0].dtype:
+            raise TypeError("all operands must share one value dtype")
+    a_row = np.concatenate([[0], np.cumsum([a.m for a in As])]).astype(np.int32)
+    b_row = np.concatenate([[0], np.cumsum([b.m for b in Bs])]).astype(np.int32)
+    c_col = np.concatenate([[0], np.cumsum([b.n for b in Bs])]).astype(np.int32)
+
+    def pack(mats, col_shift):
+        nnz_off = np.concatenate([[0], np.cumsum([x.nnz for x in mats])])
+        rpt = torch.cat([x.rpt[:-1] + int(nnz_off[i]) for i, x in enumerate(mats)] +
+                        [torch.tensor([int(nnz_off[-1])], dtype=torch.int32,
+                                      device=mats[0].rpt.device)])
+        col = torch.cat([x.col + int(col_shift[i]) for i, x in enumerate(mats)])
+        val = torch.cat([x.val for x in mats])
+        return rpt.to(torch.int32), col.to(torch.int32), val
+
+    ar, ac, av = pack(As, b_row)
+    br, bc, bv = pack(Bs, c_col)
+    A = DeviceCSR(int(a_row[-1]), int(b_row[-1]), ar, ac, av)
+    B = DeviceCSR(int(b_row[-1]), int(c_col[-1]), br, bc, bv)
+    return PackedBatch(a_row, b_row, c_col, A, B)
+
+
+def batch(pb: PackedBatch, handle: Handle | None = None, stream=None) -> list[DeviceCSR]:
+    """C_i = A_i * B_i for every product of a packed batch, run as one binned
+    product of the block-diagonal operands (spgemm_batch_*).  Returns one
+    DeviceCSR per product with local indices (views into shared storage)."""
+    _require_torch()
+    h = handle or default_handle()
+    desc = N.BatchDesc(pb.count, pb.a_row_off.ctypes.data, pb.b_row_off.ctypes.data,
+                       pb.c_col_off.ctypes.data)
+    out = N.BatchOut()
+    va, vb = pb.A.view(), pb.B.view()
+    fn = N.lib().spgemm_batch_f64 if pb.A.dtype == torch.float64 else N.lib().spgemm_batch_f32
+    N.check(fn(h.ptr, C.byref(desc), C.byref(va), C.byref(vb), C.byref(out),
+               _stream_ptr(stream)))
+    h._last_groups = int(out.n_groups)
+    owner = _BatchOwner(out)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    vt = "<f8" if pb.A.dtype == torch.float64 else "<f4"
+    res = []
+    for i in range(out.count):
+        p = out.products[i]
+        rpt = torch.as_tensor(_LibraryArray(owner, p.rpt, p.m + 1, "<i4"), device=dev)
+        if p.nnz > 0:
+            col = torch.as_tensor(_LibraryArray(owner, p.col, p.nnz, "<i4"), device=dev)
+            val = torch.as_tensor(_LibraryArray(owner, p.val, p.nnz, vt), device=dev)
+        else:
+            col = torch.empty(0, dtype=torch.int32, device=dev)
+            val = torch.empty(0, dtype=pb.A.dtype, device=dev)
+        res.append(DeviceCSR(int(p.m), int(p.n), rpt, col, val))
+    return res
+
+
+def batch_groups(handle: Handle) -> int:
+    """Groups the last batch on `handle` ran as (kept for reporting)."""
+    return getattr(handle, "_last_groups", -1)
+
+
 def _host_view(a: HostCSR) -> tuple[N.CsrView, list]:
     keep = [np.ascontiguousarray(a.rpt, dtype=np.int32),
             np.ascontiguousarray(a.col, dtype=np.int32),

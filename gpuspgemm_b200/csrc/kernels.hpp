@@ -104,6 +104,13 @@ cudaError_t launch_bin_scatter(int32_t* c_rpt, int32_t m, const int32_t* hist_of
 // Operand validation (checked mode).
 cudaError_t launch_check_csr(const int32_t* rpt, const int32_t* col, int32_t m, int32_t n,
                              int32_t nnz, DevStatus* st, cudaStream_t s);
+// Batched form (k_batch.cu): NIP per product; per-product split of a group's C.
+cudaError_t launch_product_nip(const int32_t* a_rpt, const int32_t* a_col, const int32_t* b_rpt,
+                               const int32_t* row_off, int32_t count, long long* nip,
+                               cudaStream_t s);
+cudaError_t launch_unpack(const int32_t* c_rpt, int32_t* c_col, const int32_t* row_off,
+                          const int32_t* col_off, const int64_t* out_off, int32_t first,
+                          int32_t count, int32_t* rpt_out, int32_t* pos_out, cudaStream_t s);
 // Total NIP only (spgemm_get_nip).
 cudaError_t launch_total_nip(const int32_t* a_rpt, const int32_t* a_col, const int32_t* b_rpt,
                              int32_t m, long long* out, cudaStream_t s);

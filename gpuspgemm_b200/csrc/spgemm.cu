@@ -560,6 +560,196 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     return SPGEMM_OK;
 }
 
+// ---- batched products -------------------------------------------------------
+// C_i = A_i * B_i for every product of a block-diagonal batch: the products
+// are grouped so that each group's intermediate products (an upper bound of its
+// nnz) stay below 2^31, and each group runs as ONE product of the row range of
+// the packed operands -- its rows share bins, kernels and side streams.  A
+// split kernel then gives every product its own row pointer (from 0) and local
+// column indices, as views into the group's arrays.
+template<typename V>
+spgemm_status batch(spgemm_handle_s* h, const spgemm_batch_desc* d, const spgemm_csr_view* A,
+                    const spgemm_csr_view* B, spgemm_batch_out* out, cudaStream_t stream) {
+    if (h == nullptr || d == nullptr || out == nullptr)
+        return fail(SPGEMM_ERR_INVALID_ARG, "NULL argument");
+    std::memset(out, 0, sizeof(*out));
+    if (spgemm_status st = check_view(A, "A"); st != SPGEMM_OK) return st;
+    if (spgemm_status st = check_view(B, "B"); st != SPGEMM_OK) return st;
+    const int32_t count = d->count;
+    if (count < 0) return fail(SPGEMM_ERR_INVALID_ARG, "negative batch count");
+    if (count == 0) return SPGEMM_OK;
+    if (d->a_row_off == nullptr || d->b_row_off == nullptr || d->c_col_off == nullptr)
+        return fail(SPGEMM_ERR_INVALID_ARG, "NULL batch offset array");
+    if (A->n != B->m) return fail(SPGEMM_ERR_INVALID_ARG, "A.n must equal B.m");
+    if (d->a_row_off[0] != 0 || d->b_row_off[0] != 0 || d->c_col_off[0] != 0 ||
+        d->a_row_off[count] != A->m || d->b_row_off[count] != B->m ||
+        d->c_col_off[count] != B->n)
+        return fail(SPGEMM_ERR_INVALID_ARG,
+                    "batch offsets must start at 0 and end at A.m, B.m and B.n");
+    for (int i = 0; i < count; i++)
+        if (d->a_row_off[i + 1] < d->a_row_off[i] || d->b_row_off[i + 1] < d->b_row_off[i] ||
+            d->c_col_off[i + 1] < d->c_col_off[i])
+            return fail(SPGEMM_ERR_INVALID_ARG, "batch offsets must be non-decreasing");
+    B200_TRY(cudaSetDevice(h->device));
+
+    // per-product output row-pointer offsets: product i starts at a_row_off[i] + i
+    std::vector<int64_t> out_off(count + 1);
+    for (int i = 0; i <= count; i++) out_off[i] = int64_t(d->a_row_off[i]) + i;
+
+    // device copies of the offsets, the per-product NIP, and the split results
+    const size_t nb_row = sizeof(int32_t) * (size_t(count) + 1);
+    const size_t nb_off = sizeof(int64_t) * (size_t(count) + 1);
+    const size_t nb_nip = sizeof(long long) * size_t(count);
+    const size_t nb_pos = sizeof(int32_t) * 2 * size_t(count);
+    const size_t o_row = 0;
+    const size_t o_col = align_up(o_row + nb_row, 256);
+    const size_t o_off = align_up(o_col + nb_row, 256);
+    const size_t o_nip = align_up(o_off + nb_off, 256);
+    const size_t o_pos = align_up(o_nip + nb_nip, 256);
+    const size_t total = align_up(o_pos + nb_pos, 256);
+    char* dbuf = nullptr;
+    B200_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&dbuf), total, h->pool, stream));
+    auto release = [&]() { cudaFreeAsync(dbuf, stream); };
+    int32_t* d_row = reinterpret_cast<int32_t*>(dbuf + o_row);
+    int32_t* d_col = reinterpret_cast<int32_t*>(dbuf + o_col);
+    int64_t* d_off = reinterpret_cast<int64_t*>(dbuf + o_off);
+    long long* d_nip = reinterpret_cast<long long*>(dbuf + o_nip);
+    int32_t* d_pos = reinterpret_cast<int32_t*>(dbuf + o_pos);
+    std::vector<long long> nip(count);
+    cudaError_t e = cudaMemcpyAsync(d_row, d->a_row_off, nb_row, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_col, d->c_col_off, nb_row, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_off, out_off.data(), nb_off, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = launch_product_nip(A->rpt, A->col, B->rpt, d_row, count, d_nip, stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(nip.data(), d_nip, nb_nip, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        release();
+        return cuda_fail(e, "batch planning");
+    }
+
+    // the per-product row pointers of all products share one allocation
+    int32_t* rpt_out = nullptr;
+    e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&rpt_out),
+                                sizeof(int32_t) * size_t(out_off[count]), h->pool, stream);
+    if (e != cudaSuccess) {
+        release();
+        return cuda_fail(e, "allocate batch row pointers");
+    }
+    std::vector<void*> blocks{rpt_out};
+    std::vector<spgemm_csr_out> prods(count);
+    auto unwind = [&](spgemm_status st) {
+        const std::string msg = g_last_error;
+        for (void* b : blocks) cudaFreeAsync(b, stream);
+        release();
+        cudaStreamSynchronize(stream);
+        g_last_error = msg;
+        return st;
+    };
+
+    const int saved_checked = h->checked;
+    h->checked = 0;  // group views start mid-matrix; the packed operands are checked once
+    if (saved_checked) {
+        Scratch sc;
+        if (spgemm_status st = ensure_scratch(h, std::max(A->m, B->m), &sc); st != SPGEMM_OK) {
+            h->checked = saved_checked;
+            return unwind(st);
+        }
+        cudaMemsetAsync(sc.status, 0, sizeof(DevStatus), stream);
+        e = launch_check_csr(A->rpt, A->col, A->m, A->n, A->nnz, sc.status, stream);
+        if (e == cudaSuccess) e = launch_check_csr(B->rpt, B->col, B->m, B->n, B->nnz, sc.status, stream);
+        spgemm_status st = e == cudaSuccess ? sync_mirror(h, stream, sc.plan1, sc) : cuda_fail(e, "check");
+        if (st == SPGEMM_OK) st = status_to_error(h->mirror->status);
+        if (st != SPGEMM_OK) {
+            h->checked = saved_checked;
+            return unwind(st);
+        }
+    }
+
+    constexpr long long kGroupLimit = INT32_MAX;
+    int32_t groups = 0;
+    spgemm_info acc = {};
+    for (int p0 = 0; p0 < count;) {
+        long long sum = 0;
+        int p1 = p0;
+        while (p1 < count && (p1 == p0 || sum + nip[p1] <= kGroupLimit)) sum += nip[p1++];
+        const int32_t r0 = d->a_row_off[p0];
+        const int32_t r1 = d->a_row_off[p1];
+        spgemm_csr_view Ag = *A;
+        Ag.m = r1 - r0;
+        Ag.rpt = A->rpt + r0;
+        spgemm_csr_out Cg;
+        spgemm_status st = product<V>(h, &Ag, B, &Cg, stream);
+        if (st != SPGEMM_OK) {
+            h->checked = saved_checked;
+            return unwind(st);
+        }
+        groups++;
+        acc.nip += h->info.nip;
+        acc.nnz += h->info.nnz;
+        acc.host_syncs += h->info.host_syncs;
+        acc.max_row_nip = std::max(acc.max_row_nip, h->info.max_row_nip);
+        acc.max_row_nnz = std::max(acc.max_row_nnz, h->info.max_row_nnz);
+        for (int b = 0; b < 16; b++) {
+            acc.sym_bin_rows[b] += h->info.sym_bin_rows[b];
+            acc.num_bin_rows[b] += h->info.num_bin_rows[b];
+        }
+        if (Cg.col) blocks.push_back(Cg.col);
+        if (Cg.val) blocks.push_back(Cg.val);
+        e = launch_unpack(Cg.rpt, Cg.col, d_row, d_col, d_off, p0, p1 - p0, rpt_out, d_pos,
+                          stream);
+        if (e == cudaSuccess) e = cudaFreeAsync(Cg.rpt, stream);  // split copies what it needs
+        if (e != cudaSuccess) {
+            h->checked = saved_checked;
+            return unwind(cuda_fail(e, "batch split"));
+        }
+        for (int i = p0; i < p1; i++) {
+            prods[i].m = d->a_row_off[i + 1] - d->a_row_off[i];
+            prods[i].n = d->c_col_off[i + 1] - d->c_col_off[i];
+            prods[i].rpt = rpt_out + out_off[i];
+            prods[i].col = Cg.col;  // offset added once the positions are back
+            prods[i].val = Cg.val;
+        }
+        p0 = p1;
+    }
+    h->checked = saved_checked;
+    std::vector<int32_t> pos(2 * size_t(count));
+    e = cudaMemcpyAsync(pos.data(), d_pos, nb_pos, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return unwind(cuda_fail(e, "batch positions"));
+    for (int i = 0; i < count; i++) {
+        prods[i].nnz = pos[2 * i + 1];
+        if (prods[i].col) {
+            prods[i].col += pos[2 * i];
+            prods[i].val = static_cast<V*>(prods[i].val) + pos[2 * i];
+        }
+        if (prods[i].nnz == 0) {
+            prods[i].col = nullptr;
+            prods[i].val = nullptr;
+        }
+    }
+    release();
+    acc.n_sym_bins = h->info.n_sym_bins;
+    acc.n_num_bins = h->info.n_num_bins;
+    h->info = acc;
+    out->count = count;
+    out->products = static_cast<spgemm_csr_out*>(std::malloc(sizeof(spgemm_csr_out) * count));
+    out->blocks = static_cast<void**>(std::malloc(sizeof(void*) * blocks.size()));
+    if (out->products == nullptr || out->blocks == nullptr) {
+        std::free(out->products);
+        std::free(out->blocks);
+        std::memset(out, 0, sizeof(*out));
+        return unwind(fail(SPGEMM_ERR_OOM, "host allocation of the batch result"));
+    }
+    std::memcpy(out->products, prods.data(), sizeof(spgemm_csr_out) * count);
+    std::memcpy(out->blocks, blocks.data(), sizeof(void*) * blocks.size());
+    out->n_blocks = static_cast<int32_t>(blocks.size());
+    out->n_groups = groups;
+    return SPGEMM_OK;
+}
+
 // Page-locked host blocks for host results, reused across calls (process
 // wide, so spgemm_host_csr_free needs no handle).  A result's three arrays
 // share one block; freeing the result returns the block to the pool.
@@ -784,6 +974,33 @@ spgemm_status spgemm_csr_host_f64(spgemm_handle_t h, const spgemm_csr_view* A,
 spgemm_status spgemm_csr_host_f32(spgemm_handle_t h, const spgemm_csr_view* A,
                                   const spgemm_csr_view* B, spgemm_csr_out* C, void* stream) {
     return product_host<float>(h, A, B, C, static_cast<cudaStream_t>(stream));
+}
+
+spgemm_status spgemm_batch_f64(spgemm_handle_t h, const spgemm_batch_desc* d,
+                               const spgemm_csr_view* A, const spgemm_csr_view* B,
+                               spgemm_batch_out* out, void* stream) {
+    return batch<double>(h, d, A, B, out, static_cast<cudaStream_t>(stream));
+}
+
+spgemm_status spgemm_batch_f32(spgemm_handle_t h, const spgemm_batch_desc* d,
+                               const spgemm_csr_view* A, const spgemm_csr_view* B,
+                               spgemm_batch_out* out, void* stream) {
+    return batch<float>(h, d, A, B, out, static_cast<cudaStream_t>(stream));
+}
+
+spgemm_status spgemm_batch_free(spgemm_batch_out* out, void* stream) {
+    if (out == nullptr) return SPGEMM_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaSuccess;
+    for (int32_t i = 0; i < out->n_blocks; i++) {
+        const cudaError_t ei = cudaFreeAsync(out->blocks[i], s);
+        if (e == cudaSuccess) e = ei;
+    }
+    std::free(out->blocks);
+    std::free(out->products);
+    std::memset(out, 0, sizeof(*out));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFreeAsync");
+    return SPGEMM_OK;
 }
 
 spgemm_status spgemm_csr_free(spgemm_csr_out* C, void* stream) {

@@ -226,3 +226,57 @@ def _poisson_square(n: int, lam: float, seed: int, dtype) -> HostCSR:
     rows, cols = sample_distinct_per_row(rng, counts, n)
     vals = rng.uniform(-1.0, 1.0, size=rows.shape[0])
     return _from_row_keys(n, n, rows, cols, vals, dtype)
+
+
+def batch_packed_gpu(count: int = 4096, seed: int = DEFAULT_SEED, dtype=None, device="cuda",
+                     rows_lo: int = 64, rows_hi: int = 16384, lam_lo: float = 6.0,
+                     lam_hi: float = 40.0):
+    """The batched workload generated directly on the GPU in packed form.
+
+    `count` independent square pairs (A_i, B_i): rows log-uniform in
+    [rows_lo, rows_hi], nnz per row ~ Poisson(lambda_i) with lambda_i ~
+    U[lam_lo, lam_hi] (capped at the row count), uniform random columns with
+    duplicates within a row dropped, values U[-1, 1].  Returns
+    (a_row_off, b_row_off, c_col_off, A_packed, B_packed) with block-diagonal
+    operands in global column indices (gpuspgemm_b200.api.PackedBatch fields).
+    Seeded: sizes and rates from numpy, entries from a seeded torch generator on
+    the device.
+    """
+    import torch
+    dtype = dtype or torch.float32
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(rows_lo), np.log(rows_hi), size=count)).astype(np.int64)
+    lams = rng.uniform(lam_lo, lam_hi, size=count)
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    if off[-1] >= 2**31:
+        raise ValueError("batch has too many rows for int32 indices")
+    gen = torch.Generator(device=device)
+    gen.manual_seed(int(seed) & 0x7FFFFFFF)
+    dev = torch.device(device)
+    prod_of_row = torch.repeat_interleave(torch.arange(count, device=dev),
+                                          torch.as_tensor(sizes, device=dev))
+    m_of_row = torch.as_tensor(sizes, device=dev)[prod_of_row]
+    off_of_row = torch.as_tensor(off[:-1], device=dev)[prod_of_row]
+
+    def one():
+        lam = torch.as_tensor(lams, device=dev, dtype=torch.float32)[prod_of_row]
+        cnt = torch.minimum(torch.poisson(lam, generator=gen).to(torch.int64), m_of_row)
+        rows = torch.repeat_interleave(torch.arange(int(off[-1]), device=dev), cnt)
+        u = torch.rand(rows.shape[0], device=dev, generator=gen, dtype=torch.float64)
+        col = (u * m_of_row[rows].to(torch.float64)).to(torch.int64)
+        key = rows * 16384 + col
+        key = torch.unique(key)  # sorted, duplicates dropped
+        rows = key // 16384
+        col = key % 16384
+        rpt = torch.zeros(int(off[-1]) + 1, dtype=torch.int64, device=dev)
+        rpt[1:] = torch.cumsum(torch.bincount(rows, minlength=int(off[-1])), 0)
+        gcol = col + off_of_row[rows]
+        val = (torch.rand(key.shape[0], device=dev, generator=gen, dtype=torch.float64) * 2 - 1)
+        return rpt.to(torch.int32), gcol.to(torch.int32), val.to(dtype)
+
+    from .api import DeviceCSR
+    ar, ac, av = one()
+    br, bc, bv = one()
+    n = int(off[-1])
+    offs = off.astype(np.int32)
+    return offs, offs.copy(), offs.copy(), DeviceCSR(n, n, ar, ac, av), DeviceCSR(n, n, br, bc, bv)

@@ -193,6 +193,48 @@ SPGEMM_API spgemm_status spgemm_last_profile(spgemm_handle_t handle, spgemm_kern
 SPGEMM_API spgemm_status spgemm_ladder_info(spgemm_handle_t handle, int which /*0 sym, 1 num*/,
                                  int dtype_bytes, int* n_bins, int64_t* limits /*[16]*/);
 
+/* ---- batched products ------------------------------------------------------ */
+
+/* A batch of `count` independent products C_i = A_i * B_i, given as two packed
+ * block-diagonal operands: A = blockdiag(A_0, A_1, ...), B = blockdiag(B_0, ...).
+ * Product i owns
+ *   rows    [a_row_off[i], a_row_off[i+1]) of A (and of C),
+ *   columns [b_row_off[i], b_row_off[i+1]) of A = rows of B,
+ *   columns [c_col_off[i], c_col_off[i+1]) of B (and of C);
+ * A_i's and B_i's column indices are global (already shifted by those offsets),
+ * so the packed operands are ordinary CSR matrices.  All three offset arrays
+ * are HOST arrays of count + 1 entries.  No counterpart in the reference, which
+ * multiplies one pair per call. */
+typedef struct spgemm_batch_desc {
+    int32_t count;
+    const int32_t* a_row_off;
+    const int32_t* b_row_off;
+    const int32_t* c_col_off;
+} spgemm_batch_desc;
+
+/* Result of a batch: one CSR per product, with LOCAL indices (row pointer from
+ * 0, columns in [0, n_i)), as views into a few device allocations.  `products`
+ * is a host array of `count` entries; `blocks` lists the device allocations. */
+typedef struct spgemm_batch_out {
+    int32_t count;
+    spgemm_csr_out* products;
+    int32_t n_blocks;
+    void** blocks;
+    int32_t n_groups;  /* block-diagonal sub-products the batch was run as */
+} spgemm_batch_out;
+
+/* Run the batch as one binned product of the block-diagonal operands (split
+ * into as few groups as int32 nnz allows: each group's intermediate products
+ * stay below 2^31), so rows of every product share bins, kernels and streams
+ * instead of one launch sequence per product.  Synchronous on return. */
+SPGEMM_API spgemm_status spgemm_batch_f64(spgemm_handle_t handle, const spgemm_batch_desc* desc,
+                                          const spgemm_csr_view* A, const spgemm_csr_view* B,
+                                          spgemm_batch_out* out, void* stream);
+SPGEMM_API spgemm_status spgemm_batch_f32(spgemm_handle_t handle, const spgemm_batch_desc* desc,
+                                          const spgemm_csr_view* A, const spgemm_csr_view* B,
+                                          spgemm_batch_out* out, void* stream);
+SPGEMM_API spgemm_status spgemm_batch_free(spgemm_batch_out* out, void* stream);
+
 /* ---- allocation-free row sizes --------------------------------------------- */
 
 /* Largest B.n that spgemm_row_nnz_noalloc accepts. */

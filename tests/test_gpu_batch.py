@@ -1,0 +1,71 @@
+"""GPU: the batched form (spgemm_batch_*) -- many independent products run as
+one binned product of block-diagonal operands.  Every product of the batch must
+equal the same product run alone (structure bit-exact) and the CPU oracle
+(values within tolerance)."""
+import numpy as np
+import pytest
+
+from gpuspgemm_b200 import generators as G
+from gpuspgemm_b200.csr import HostCSR
+
+pytestmark = pytest.mark.gpu
+
+
+def _host(d) -> HostCSR:
+    return d.to_host()
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_batch_matches_oracle_and_single_calls(handle, oracle_mod, dtype):
+    import torch
+
+    from gpuspgemm_b200.api import DeviceCSR, batch, pack_batch, proposal
+    pairs_h = list(G.batch_pairs(24, seed=91, dtype=dtype, rows_lo=16, rows_hi=2000))
+    # rectangular and empty members too
+    pairs_h.append((G.uniform_rows(300, 5, seed=92, m=120).astype(dtype),
+                    G.uniform_rows(70, 4, seed=93, m=300).astype(dtype)))
+    pairs_h.append((HostCSR(5, 3, np.zeros(6, np.int32), np.zeros(0, np.int32),
+                            np.zeros(0, dtype)),
+                    G.uniform_rows(4, 2, seed=94, m=3).astype(dtype)))
+    pairs = [(DeviceCSR.from_host(a), DeviceCSR.from_host(b)) for a, b in pairs_h]
+    pb = pack_batch(pairs)
+    out = batch(pb, handle)
+    assert len(out) == len(pairs)
+    tol = 1e-12 if dtype == np.float64 else 1e-5
+    for (a, b), (da, db), c in zip(pairs_h, pairs, out):
+        ch = _host(c)
+        assert (ch.m, ch.n) == (a.m, b.n)
+        single = proposal(da, db, handle).to_host()
+        assert np.array_equal(ch.rpt, single.rpt) and np.array_equal(ch.col, single.col)
+        a64, b64 = a.astype(np.float64), b.astype(np.float64)
+        R = oracle_mod.spgemm(a64, b64, np.float64)
+        res = oracle_mod.compare(ch, R, oracle_mod.abs_bound(a64, b64, R))
+        assert res["rpt_equal"] and res["col_equal"], res
+        assert res.get("max_cond", 0.0) <= tol, res
+    torch.cuda.synchronize()
+
+
+def test_batch_packed_gpu_generator_and_groups(handle, oracle_mod):
+    import torch
+
+    from gpuspgemm_b200.api import PackedBatch, batch
+    a_off, b_off, c_off, A, B = G.batch_packed_gpu(40, seed=95, rows_lo=64, rows_hi=3000)
+    pb = PackedBatch(a_off, b_off, c_off, A, B)
+    out = batch(pb, handle)
+    Ah, Bh = A.to_host(), B.to_host()
+    for i in (0, 7, 39):
+        r0, r1 = int(a_off[i]), int(a_off[i + 1])
+        # product i alone on the CPU, in local indices
+        rpt = Ah.rpt[r0:r1 + 1] - Ah.rpt[r0]
+        Ai = HostCSR(r1 - r0, r1 - r0, rpt, Ah.col[Ah.rpt[r0]:Ah.rpt[r1]] - r0,
+                     Ah.val[Ah.rpt[r0]:Ah.rpt[r1]].astype(np.float64))
+        rptb = Bh.rpt[r0:r1 + 1] - Bh.rpt[r0]
+        Bi = HostCSR(r1 - r0, r1 - r0, rptb, Bh.col[Bh.rpt[r0]:Bh.rpt[r1]] - r0,
+                     Bh.val[Bh.rpt[r0]:Bh.rpt[r1]].astype(np.float64))
+        R = oracle_mod.spgemm(Ai, Bi, np.float64)
+        ch = out[i].to_host()
+        res = oracle_mod.compare(ch, R, oracle_mod.abs_bound(Ai, Bi, R))
+        assert res["rpt_equal"] and res["col_equal"], res
+        assert res["max_cond"] <= 1e-5, res
+    assert handle._last_groups >= 1
+    torch.cuda.synchronize()
