@@ -53,10 +53,13 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--out", type=str, default="")
-    ap.add_argument("--mode", choices=["plain", "batch"], default="plain",
+    ap.add_argument("--mode", choices=["plain", "batch", "served"], default="plain",
                     help="plain: the headline C=A*A workload; batch: many independent "
                          "products (batched form vs one call per product)")
     ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--requests", type=int, default=600)
+    ap.add_argument("--load", type=float, default=0.8,
+                    help="served mode: offered load as a fraction of the plain path's capacity")
     return ap.parse_args()
 
 
@@ -318,7 +321,7 @@ def run_ours(args, rank, world, local_rank):
     nip_rows[nz] = np.add.reduceat(contrib, A.rpt[:-1][nz])
     nnz_rows = np.diff(c_rpt).astype(np.int64)
     if phase == 3:
-        lim = h.ladder(1, s_bytes)
+        lim = h.ladder(2 if A.n <= (1 << 20) else 1, s_bytes)
         keys = nnz_rows
         numeric, write_c = True, True
     elif phase == 1:
@@ -450,6 +453,142 @@ def run_batch(args, local_rank):
     }
 
 
+# ---- served form: Poisson arrivals of mixed-size requests ----------------------
+
+def served_pool(seed: int):
+    """Device-resident operand pools of the served stream (FP64): 70 % small
+    (<= 16k rows, Poisson(12) nnz/row), 25 % medium (<= 256k rows, Zipf(2.0)
+    degrees as in the 1M power-law, cap scaled down), 5 % large (the 1M
+    power-law itself)."""
+    from gpuspgemm_b200 import generators as G
+    from gpuspgemm_b200.api import DeviceCSR
+    rng = np.random.default_rng(seed)
+    small = [G._poisson_square(int(np.exp(rng.uniform(np.log(256), np.log(16384)))), 12.0,
+                               seed + 1 + i, np.float64) for i in range(48)]
+    medium = [G.power_law(int(n), 2.0, max(50, int(4700 * n / 1_000_000)), seed=seed + 100 + i)
+              for i, n in enumerate(rng.integers(64_000, 256_001, size=6))]
+    large = [G.power_law(1_000_000, 2.0, 4700, seed=seed)]
+    return [[DeviceCSR.from_host(a) for a in pool] for pool in (small, medium, large)]
+
+
+def run_served(args, local_rank):
+    import time as _t
+
+    import torch
+
+    from gpuspgemm_b200.api import Handle, proposal
+    from gpuspgemm_b200.serve import SpgemmServer, latency_summary
+
+    torch.cuda.set_device(local_rank)
+    pools = served_pool(args.seed)
+    rng = np.random.default_rng(args.seed + 7)
+    kinds = rng.choice(3, size=args.requests, p=[0.70, 0.25, 0.05])
+    picks = [pools[k][int(rng.integers(len(pools[k])))] for k in kinds]
+    h = Handle(local_rank)
+    # isolated solve time of every distinct operand (warm), and its NIP
+    iso = {}
+    nips = {}
+    for pool in pools:
+        for d in pool:
+            proposal(d, d, h)
+            torch.cuda.synchronize()
+            t0 = _t.perf_counter()
+            proposal(d, d, h)
+            torch.cuda.synchronize()
+            iso[id(d)] = _t.perf_counter() - t0
+            nips[id(d)] = h.info()["nip"]
+    iso_times = np.array([iso[id(d)] for d in picks])
+    total_nip = int(sum(nips[id(d)] for d in picks))
+    plain_capacity = len(picks) / iso_times.sum()           # requests/s, one call at a time
+
+    def plain_fifo(arrivals):
+        """One request at a time, in arrival order (the plain path as a server)."""
+        lat = []
+        t_start = _t.perf_counter()
+        for d, ta in zip(picks, arrivals):
+            now = _t.perf_counter() - t_start
+            if now < ta:
+                _t.sleep(ta - now)
+            proposal(d, d, h)
+            torch.cuda.synchronize()
+            lat.append(_t.perf_counter() - t_start - ta)
+        return np.array(lat), _t.perf_counter() - t_start
+
+    def served(arrivals):
+        server = SpgemmServer(memory_budget=48 << 30, max_batch=256, workers=2,
+                              device=local_rank)
+        reqs = []
+        t_start = _t.perf_counter()
+        for d, ta in zip(picks, arrivals):
+            now = _t.perf_counter() - t_start
+            if now < ta:
+                _t.sleep(ta - now)
+            reqs.append(server.submit(d, d, t_arrival=t_start + ta))
+        for r in reqs:
+            r.done.wait()
+        span = max(r.t_done for r in reqs) - t_start
+        bad = [r for r in reqs if r.error is not None]
+        tl = server.timeline
+        batches = {"units": len(tl), "batched": sum(1 for u in tl if u[1] > 1),
+                   "alone": sum(1 for u in tl if u[1] == 1),
+                   "largest_batch": max((u[1] for u in tl), default=0)}
+        server.close()
+        if bad:
+            raise bad[0].error
+        return reqs, span, batches
+
+    def median_run(fn, key):
+        runs = sorted((fn() for _ in range(3)), key=key)
+        return runs[1]
+
+    # saturation: every request present at t = 0 (median of 3 runs each)
+    zero = np.zeros(len(picks))
+    served(zero[: min(32, len(picks))])  # warm the server's handles
+    reqs_sat, span_sat, batches_sat = median_run(lambda: served(zero), key=lambda r: r[1])
+    _, span_plain_sat = median_run(lambda: plain_fifo(zero), key=lambda r: r[1])
+    # fixed offered load: Poisson arrivals at `load` x the plain path's capacity;
+    # the run with the median p99 latency of 3
+    rate = args.load * plain_capacity
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(picks)))
+    reqs_load, span_load, batches_load = median_run(
+        lambda: served(arrivals), key=lambda r: latency_summary(r[0])["p99_ms"])
+    lat_plain, _ = median_run(lambda: plain_fifo(arrivals),
+                              key=lambda r: float(np.percentile(r[0], 99)))
+    h.close()
+    s_load = latency_summary(reqs_load)
+    by_kind = {name: latency_summary([r for r, k in zip(reqs_load, kinds) if k == i])
+               for i, name in enumerate(["small", "medium", "large"]) if (kinds == i).any()}
+    plain_by_kind = {name: {"p50_ms": float(np.percentile(lat_plain[kinds == i], 50) * 1e3),
+                            "p99_ms": float(np.percentile(lat_plain[kinds == i], 99) * 1e3)}
+                     for i, name in enumerate(["small", "medium", "large"]) if (kinds == i).any()}
+    iso_p99 = float(np.percentile(iso_times, 99) * 1e3)
+    return {
+        "metric": "served mixed SpGEMM stream: products/s at saturation, p50/p99 latency at "
+                  f"{args.load:.0%} of the plain path's capacity",
+        "value": len(picks) / span_sat, "unit": "products/s", "n_gpus": 1,
+        "steps": 3, "warmup": 1, "ms_per_step": span_sat * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded): 70% small Poisson(12) rows <=16k, 25% medium power-law "
+                "<=256k rows, 5% the 1M power-law",
+        "config": {"requests": len(picks), "mix": {k: int((kinds == i).sum()) for i, k in
+                                                   enumerate(["small", "medium", "large"])},
+                   "nip_total": total_nip, "memory_budget_bytes": 48 << 30, "workers": 2},
+        "saturation": {"served_products_per_s": len(picks) / span_sat,
+                       "plain_products_per_s": len(picks) / span_plain_sat,
+                       "speedup": span_plain_sat / span_sat,
+                       "served_gflops": 2.0 * total_nip / span_sat / 1e9,
+                       "batches": batches_sat},
+        "at_load": {"offered_per_s": rate, "served": s_load, "served_by_kind": by_kind,
+                    "plain_fifo_by_kind": plain_by_kind,
+                    "plain_fifo": {"p50_ms": float(np.percentile(lat_plain, 50) * 1e3),
+                                   "p99_ms": float(np.percentile(lat_plain, 99) * 1e3)},
+                    "batches": batches_load,
+                    "served_products_per_s": len(picks) / span_load},
+        "isolated": {"p50_ms": float(np.percentile(iso_times, 50) * 1e3), "p99_ms": iso_p99},
+        "p99_served_over_p99_isolated": s_load["p99_ms"] / iso_p99,
+    }
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -457,6 +596,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.mode == "batch":
         line = run_batch(args, local_rank) if rank == 0 else None
+    elif args.mode == "served":
+        line = run_served(args, local_rank) if rank == 0 else None
     elif args.impl == "reference":
         line = run_reference(args, rank)
     else:

@@ -252,8 +252,12 @@ class PackedBatch:
 
 
 def pack_batch(pairs) -> PackedBatch:
-    """Pack [(A_i, B_i)] (DeviceCSR, A_i.n == B_i.m) into block-diagonal operands."""
-    _require_torch()
+    """Pack [(A_i, B_i)] (DeviceCSR, A_i.n == B_i.m) into block-diagonal operands
+    on the operands' device (host logic plus torch ops; no library call)."""
+    if torch is None:
+        raise RuntimeError("torch is required")
+    if not pairs:
+        raise ValueError("empty batch")
     As = [a for a, _ in pairs]
     Bs = [b for _, b in pairs]
     for a, b in pairs:
@@ -265,14 +269,29 @@ def pack_batch(pairs) -> PackedBatch:
     b_row = np.concatenate([[0], np.cumsum([b.m for b in Bs])]).astype(np.int32)
     c_col = np.concatenate([[0], np.cumsum([b.n for b in Bs])]).astype(np.int32)
 
+    dev = As[0].rpt.device
+
     def pack(mats, col_shift):
-        nnz_off = np.concatenate([[0], np.cumsum([x.nnz for x in mats])])
-        rpt = torch.cat([x.rpt[:-1] + int(nnz_off[i]) for i, x in enumerate(mats)] +
-                        [torch.tensor([int(nnz_off[-1])], dtype=torch.int32,
-                                      device=mats[0].rpt.device)])
-        col = torch.cat([x.col + int(col_shift[i]) for i, x in enumerate(mats)])
+        # one concatenation per array; the per-matrix offsets are expanded on
+        # the device (repeat_interleave with a known output size: no host sync,
+        # nothing nnz-sized on the host).  Packed sizes fit int32 (checked by
+        # the caller's row/column sums and by the library).
+        nnz = np.array([x.nnz for x in mats], np.int64)
+        rows = np.array([x.m for x in mats], np.int64)
+        tot_nnz = int(nnz.sum())
+        if tot_nnz > np.iinfo(np.int32).max:
+            raise ValueError("packed operand has more than 2^31-1 entries")
+        small = torch.from_numpy(np.stack([np.cumsum(nnz) - nnz, col_shift[:-1].astype(np.int64),
+                                           rows, nnz])).to(dev, non_blocking=True)
+        rpt = torch.empty(int(rows.sum()) + 1, dtype=torch.int32, device=dev)
+        torch.cat([x.rpt[:-1] for x in mats], out=rpt[:-1])
+        rpt[:-1] += torch.repeat_interleave(small[0].to(torch.int32), small[2],
+                                            output_size=int(rows.sum()))
+        rpt[-1] = tot_nnz
+        col = torch.cat([x.col for x in mats])
+        col += torch.repeat_interleave(small[1].to(torch.int32), small[3], output_size=tot_nnz)
         val = torch.cat([x.val for x in mats])
-        return rpt.to(torch.int32), col.to(torch.int32), val
+        return rpt, col, val
 
     ar, ac, av = pack(As, b_row)
     br, bc, bv = pack(Bs, c_col)

@@ -103,6 +103,50 @@ __device__ __forceinline__ void cta_for_products(const int32_t* __restrict__ a_c
     }
 }
 
+// Column window of one row of C: the smallest first column and the largest
+// last column over the B rows that the A entries [a0, a1) select, clamped to
+// [0, n_cols).  When B's rows are sorted every key of the row lies inside it;
+// callers that depend on that check each key and fall back to [0, n_cols).
+// Returns (lo, hi); lo > hi for a row with no products.  All threads must call
+// it (three barriers; it reuses sc.exc / sc.bs).
+template<int THREADS>
+__device__ __forceinline__ int2 cta_col_window(const int32_t* __restrict__ a_col,
+                                               const int32_t* __restrict__ b_rpt,
+                                               const int32_t* __restrict__ b_col, int a0, int a1,
+                                               int n_cols, CtaScratch<THREADS>& sc) {
+    constexpr int NW = THREADS / kWarp;
+    int lo = INT32_MAX;
+    int hi = -1;
+    for (int e = a0 + threadIdx.x; e < a1; e += THREADS) {
+        const int r = __ldg(a_col + e);
+        const int s0 = __ldg(b_rpt + r);
+        const int s1 = __ldg(b_rpt + r + 1);
+        if (s0 < s1) {
+            lo = min(lo, __ldg(b_col + s0));
+            hi = max(hi, __ldg(b_col + s1 - 1));
+        }
+    }
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    __syncthreads();  // the previous user of exc / bs is done
+    if (lane == 0) {
+        sc.exc[w] = lo;
+        sc.bs[w] = hi;
+    }
+    __syncthreads();
+    lo = INT32_MAX;
+    hi = -1;
+#pragma unroll
+    for (int i = 0; i < NW; i++) {
+        lo = min(lo, sc.exc[i]);
+        hi = max(hi, sc.bs[i]);
+    }
+    __syncthreads();  // exc / bs are free again for the product walk
+    return make_int2(max(lo, 0), min(hi, n_cols - 1));
+}
+
 // Move the non-empty slots of table[0, T) to its front, in slot order.
 // Returns the number of keys.  Reads of a chunk complete (barrier inside the
 // scan) before any write, and writes land at or before the slot they came

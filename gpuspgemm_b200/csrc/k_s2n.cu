@@ -123,7 +123,108 @@ __global__ __launch_bounds__(THREADS) void k_s2n_cta(ProductArgs p) {
     for (int i = threadIdx.x; i < nnz; i += THREADS) out[i] = vals[i];
 }
 
-// Global bin: bitmap of B.n bits per row in flight; the set bits, read in
+// Bitmap bin (B.n <= kBitmapCols): the row's hash table is the identity hash
+// over B's columns, one BIT per column, in shared memory (128 KB for 2^20
+// columns).  atomicOr fills it; the set bits read in word order are the sorted
+// column list, so no sort is needed.  Extraction: each warp owns a contiguous
+// run of words; warp totals are scanned across the CTA, then each warp scans
+// its 32-word chunks with shuffles and writes its columns.  The bitmap's space
+// then holds the row's values for the binary-search accumulation.
+constexpr int kBitmapWords = kBitmapCols / 32;
+
+template<typename V, int THREADS, int CAP>
+struct BitmapLayout {
+    static constexpr size_t bm_bytes = sizeof(uint32_t) * kBitmapWords;
+    static constexpr size_t region0 =
+        bm_bytes > sizeof(V) * CAP ? bm_bytes : sizeof(V) * CAP;
+    static constexpr size_t cols_bytes = sizeof(int32_t) * CAP;
+    static constexpr size_t bytes = region0 + cols_bytes + sizeof(CtaScratch<THREADS>);
+};
+
+template<typename V, int THREADS, int CAP>
+__global__ __launch_bounds__(THREADS) void k_s2n_bitmap(ProductArgs p) {
+    using L = BitmapLayout<V, THREADS, CAP>;
+    constexpr int NW = THREADS / kWarp;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t* bm = reinterpret_cast<uint32_t*>(smem_raw);
+    V* vals = reinterpret_cast<V*>(smem_raw);  // after the bitmap is read out
+    int32_t* cols = reinterpret_cast<int32_t*>(smem_raw + L::region0);
+    auto& sc = *reinterpret_cast<CtaScratch<THREADS>*>(smem_raw + L::region0 + L::cols_bytes);
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int w = tid >> 5;
+    const int row = p.rows[blockIdx.x];
+    const int c0 = p.c_rpt[row];
+    const int nnz = p.c_rpt[row + 1] - c0;
+    const int words = (p.n_cols + 31) >> 5;
+    if (nnz > CAP || words > kBitmapWords) {
+        if (tid == 0) report(p.status, kStCapacity, row, nnz);
+        return;
+    }
+    for (int i = tid; i < words; i += THREADS) bm[i] = 0u;
+    __syncthreads();
+    const int a0 = p.a_rpt[row];
+    const int a1 = p.a_rpt[row + 1];
+    cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int) {
+        const int32_t key = __ldg(p.b_col + qb);
+        atomicOr(bm + (key >> 5), 1u << (key & 31));
+    });
+    // warp w reads words [w0, w1)
+    const int seg = (words + NW - 1) / NW;
+    const int w0 = min(words, w * seg);
+    const int w1 = min(words, w0 + seg);
+    int cnt = 0;
+    for (int i = w0 + lane; i < w1; i += kWarp) cnt += __popc(bm[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0) sc.warp_tot[w] = cnt;
+    __syncthreads();
+    int base = 0;
+    int total = 0;
+#pragma unroll
+    for (int k = 0; k < NW; k++) {
+        const int t = sc.warp_tot[k];
+        base += k < w ? t : 0;
+        total += t;
+    }
+    for (int c = w0; c < w1; c += kWarp) {
+        const int i = c + lane;
+        uint32_t word = i < w1 ? bm[i] : 0u;
+        const int pc = __popc(word);
+        int inc = pc;
+#pragma unroll
+        for (int o = 1; o < kWarp; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
+        }
+        int pos = base + inc - pc;
+        while (word != 0u) {
+            const int b = __ffs(word) - 1;
+            if (pos < CAP) cols[pos] = i * 32 + b;
+            pos++;
+            word &= word - 1u;
+        }
+        base += __shfl_sync(0xffffffffu, inc, kWarp - 1);
+    }
+    __syncthreads();
+    if (total != nnz && tid == 0) report(p.status, kStCapacity, row, total);
+    for (int i = tid; i < nnz; i += THREADS) {
+        p.c_col[c0 + i] = cols[i];
+        vals[i] = V(0);
+    }
+    __syncthreads();
+    cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int ai) {
+        const int32_t key = __ldg(p.b_col + qb);
+        const int pos = lower_bound_present(cols, nnz, key);
+        atomicAdd(vals + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
+    });
+    V* out = static_cast<V*>(p.c_val) + c0;
+    for (int i = tid; i < nnz; i += THREADS) out[i] = vals[i];
+}
+
+// Global bin: a bitmap per row in flight (global scratch, B.n bits per CTA);
+// only the row's column window [lo, hi] is cleared and read, and a key outside
+// it (B rows not sorted) redoes the fill over [0, B.n).  The set bits, read in
 // word order, ARE the sorted column list.  Values accumulate with global
 // atomics after a binary search of the row's C.col in global memory
 // (the reference's k_num_global, num.cuh:251-298).
@@ -137,23 +238,44 @@ __global__ __launch_bounds__(THREADS) void k_s2n_global(ProductArgs p) {
         const int nnz = p.c_rpt[row + 1] - c0;
         const int a0 = p.a_rpt[row];
         const int a1 = p.a_rpt[row + 1];
-        for (int64_t i = threadIdx.x; i < p.words; i += THREADS) bm[i] = 0u;
-        __syncthreads();
-        cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int) {
-            const int32_t key = __ldg(p.b_col + qb);
-            atomicOr(bm + (key >> 5), 1u << (key & 31));
-        });
+        const int2 win = cta_col_window<THREADS>(p.a_col, p.b_rpt, p.b_col, a0, a1, p.n_cols, sc);
+        int lo = win.x;
+        int hi = win.y;
+        int w0 = 0;
+        int nwords = 0;
+        for (int pass = 0; pass < 2; pass++) {
+            w0 = lo >> 5;
+            nwords = hi >= lo ? (hi >> 5) - w0 + 1 : 0;
+            for (int i = threadIdx.x; i < nwords; i += THREADS) bm[i] = 0u;
+            __syncthreads();
+            int miss = 0;
+            cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int) {
+                const int32_t key = __ldg(p.b_col + qb);
+                if (key < lo || key > hi) {
+                    miss = 1;
+                    return;
+                }
+                atomicOr(bm + ((key >> 5) - w0), 1u << (key & 31));
+            });
+            if (!__syncthreads_or(miss)) break;
+            if (pass == 1) {  // a column index outside [0, B.n): keys skipped
+                if (threadIdx.x == 0) report(p.status, kStBadInput, row);
+                break;
+            }
+            lo = 0;
+            hi = p.n_cols - 1;
+        }
         int32_t* cols = p.c_col + c0;
         int base = 0;
-        for (int64_t c = 0; c < p.words; c += THREADS) {
-            const int64_t wi = c + threadIdx.x;
-            uint32_t w = wi < p.words ? bm[wi] : 0u;
+        for (int c = 0; c < nwords; c += THREADS) {
+            const int wi = c + threadIdx.x;
+            uint32_t w = wi < nwords ? bm[wi] : 0u;
             const int cnt = __popc(w);
             const int inc = block_inclusive_scan<THREADS>(cnt, sc.warp_tot);
             int pos = base + inc - cnt;
             while (w != 0u) {
                 const int b = __ffs(w) - 1;
-                if (pos < nnz) cols[pos] = static_cast<int32_t>(wi * 32 + b);
+                if (pos < nnz) cols[pos] = (w0 + wi) * 32 + b;
                 pos++;
                 w &= w - 1u;
             }
@@ -190,6 +312,13 @@ template<typename V, int THREADS, int T, int CAP>
 cudaError_t launch_cta(const ProductArgs& p, cudaStream_t s) {
     k_s2n_cta<V, THREADS, T, CAP>
         <<<p.nrows, THREADS, CtaLayout<V, THREADS, T, CAP>::bytes, s>>>(p);
+    return cudaGetLastError();
+}
+
+template<typename V, int THREADS, int CAP>
+cudaError_t launch_bitmap(const ProductArgs& p, cudaStream_t s) {
+    k_s2n_bitmap<V, THREADS, CAP>
+        <<<p.nrows, THREADS, BitmapLayout<V, THREADS, CAP>::bytes, s>>>(p);
     return cudaGetLastError();
 }
 
@@ -232,6 +361,31 @@ B200_S2N_LADDER(double)
 B200_S2N_LADDER(float)
 #undef B200_S2N_LADDER
 
+// Ladder for B.n <= kBitmapCols: rows of 3k-16k nnz use the shared-memory
+// bitmap bin instead of the hash + sort CTA bins.
+template<typename V>
+struct S2nBitmapLadder {
+    static const BinLauncher entries[];
+    static const int count;
+};
+
+#define B200_S2N_BITMAP_LADDER(V)                                                             \
+    template<>                                                                                \
+    const BinLauncher S2nBitmapLadder<V>::entries[] = {                                       \
+        S2nLadder<V>::entries[0], S2nLadder<V>::entries[1], S2nLadder<V>::entries[2],         \
+        S2nLadder<V>::entries[3], S2nLadder<V>::entries[4],                                   \
+        {BinKind::Cta, 16384, 1, 1024, BitmapLayout<V, 1024, 16384>::bytes,                   \
+         "s2n_bitmap1024", launch_bitmap<V, 1024, 16384>},                                    \
+        {BinKind::Global, INT32_MAX, 1, 1024, 0, "s2n_global_bitmap", launch_global<V, 1024>}, \
+    };                                                                                        \
+    template<>                                                                                \
+    const int S2nBitmapLadder<V>::count =                                                     \
+        sizeof(S2nBitmapLadder<V>::entries) / sizeof(BinLauncher);
+
+B200_S2N_BITMAP_LADDER(double)
+B200_S2N_BITMAP_LADDER(float)
+#undef B200_S2N_BITMAP_LADDER
+
 template<typename V>
 cudaError_t prepare_one() {
     cudaError_t e = cudaSuccess;
@@ -246,6 +400,7 @@ cudaError_t prepare_one() {
     B200_SMEM((k_s2n_cta<V, 256, 4096, 3072>), (CtaLayout<V, 256, 4096, 3072>::bytes));
     B200_SMEM((k_s2n_cta<V, 512, 16384, 12288>), (CtaLayout<V, 512, 16384, 12288>::bytes));
     B200_SMEM((k_s2n_cta<V, 1024, 20480, 16384>), (CtaLayout<V, 1024, 20480, 16384>::bytes));
+    B200_SMEM((k_s2n_bitmap<V, 1024, 16384>), (BitmapLayout<V, 1024, 16384>::bytes));
 #undef B200_SMEM
     return e;
 }
@@ -260,6 +415,16 @@ int s2n_ladder_f64(const BinLauncher** out) {
 int s2n_ladder_f32(const BinLauncher** out) {
     *out = S2nLadder<float>::entries;
     return S2nLadder<float>::count;
+}
+
+int s2n_bitmap_ladder_f64(const BinLauncher** out) {
+    *out = S2nBitmapLadder<double>::entries;
+    return S2nBitmapLadder<double>::count;
+}
+
+int s2n_bitmap_ladder_f32(const BinLauncher** out) {
+    *out = S2nBitmapLadder<float>::entries;
+    return S2nBitmapLadder<float>::count;
 }
 
 cudaError_t s2n_prepare() {

@@ -138,8 +138,11 @@ __global__ __launch_bounds__(THREADS) void k_sym1_cluster(ProductArgs p) {
     cluster.sync();  // no CTA leaves while another may still touch its table
 }
 
-// Global bin: a bitmap of B.n bits per row in flight (global scratch).
-// atomicOr tells whether a key is new; the count is exact.
+// Global bin: a bitmap per row in flight (global scratch, B.n bits per CTA),
+// of which only the row's column window [lo, hi] is cleared and used -- a
+// row of a block-diagonal batch touches one block's columns, not all of B's.
+// atomicOr tells whether a key is new; the count is exact.  A key outside
+// the window (B rows not sorted) redoes the row over [0, B.n).
 template<int THREADS>
 __global__ __launch_bounds__(THREADS) void k_sym1_global(ProductArgs p) {
     __shared__ CtaScratch<THREADS> sc;
@@ -148,19 +151,41 @@ __global__ __launch_bounds__(THREADS) void k_sym1_global(ProductArgs p) {
     const int nrows = p.nrows >= 0 ? p.nrows : *reinterpret_cast<volatile int32_t*>(p.fail_count);
     for (int rid = blockIdx.x; rid < nrows; rid += gridDim.x) {
         const int row = p.rows[rid];
-        for (int64_t i = threadIdx.x; i < p.words; i += THREADS) bm[i] = 0u;
-        __syncthreads();
-        int cnt = 0;
-        cta_for_products<THREADS>(p.a_col, p.b_rpt, p.a_rpt[row], p.a_rpt[row + 1], sc,
-                                  [&](int qb, int) {
-                                      const int32_t key = __ldg(p.b_col + qb);
-                                      const uint32_t bit = 1u << (key & 31);
-                                      const uint32_t old = atomicOr(bm + (key >> 5), bit);
-                                      cnt += (old & bit) ? 0 : 1;
-                                  });
-        cnt = block_sum<THREADS>(cnt, sc.warp_tot);
-        if (threadIdx.x == 0) p.c_rpt[row] = cnt;
-        __syncthreads();
+        const int a0 = p.a_rpt[row];
+        const int a1 = p.a_rpt[row + 1];
+        const int2 win = cta_col_window<THREADS>(p.a_col, p.b_rpt, p.b_col, a0, a1, p.n_cols, sc);
+        int lo = win.x;
+        int hi = win.y;
+        for (int pass = 0; pass < 2; pass++) {
+            const int w0 = lo >> 5;
+            const int nwords = hi >= lo ? (hi >> 5) - w0 + 1 : 0;
+            for (int i = threadIdx.x; i < nwords; i += THREADS) bm[i] = 0u;
+            __syncthreads();
+            int cnt = 0;
+            int miss = 0;
+            cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int) {
+                const int32_t key = __ldg(p.b_col + qb);
+                if (key < lo || key > hi) {
+                    miss = 1;
+                    return;
+                }
+                const uint32_t bit = 1u << (key & 31);
+                const uint32_t old = atomicOr(bm + ((key >> 5) - w0), bit);
+                cnt += (old & bit) ? 0 : 1;
+            });
+            if (!__syncthreads_or(miss)) {
+                cnt = block_sum<THREADS>(cnt, sc.warp_tot);
+                if (threadIdx.x == 0) p.c_rpt[row] = cnt;
+                __syncthreads();
+                break;
+            }
+            if (pass == 1) {  // a column index outside [0, B.n)
+                if (threadIdx.x == 0) report(p.status, kStBadInput, row);
+                break;
+            }
+            lo = 0;
+            hi = p.n_cols - 1;
+        }
     }
 }
 

@@ -74,6 +74,10 @@ int sym1_ladder(const BinLauncher** out);
 // Fused fill + sort + numeric ladder (key = nnz of the row), per value type.
 int s2n_ladder_f64(const BinLauncher** out);
 int s2n_ladder_f32(const BinLauncher** out);
+// The same for B.n <= kBitmapCols, whose large rows use a shared-memory bitmap.
+constexpr int kBitmapCols = 1 << 20;
+int s2n_bitmap_ladder_f64(const BinLauncher** out);
+int s2n_bitmap_ladder_f32(const BinLauncher** out);
 // One-time per-device attribute setup (dynamic smem opt-in) for all kernels.
 cudaError_t sym1_prepare();
 cudaError_t s2n_prepare();

@@ -106,9 +106,9 @@ struct spgemm_handle_s {
     int min_num_bin = -1;
     int cluster = 4;
     int profile = 0;
-    // C's arrays come from this stream-ordered pool; it keeps freed memory
-    // mapped (release threshold = max) so repeated products do not re-map
-    // hundreds of MB per call.  cudaFree / cudaFreeAsync release them.
+    // C's arrays come from the device's shared stream-ordered pool (see
+    // device_pool); it keeps freed memory mapped so repeated products do not
+    // re-map hundreds of MB per call.  cudaFree / cudaFreeAsync release them.
     cudaMemPool_t pool = nullptr;
     spgemm_info info = {};
     // profiling: an event pair per launch, resolved after the final sync
@@ -122,7 +122,23 @@ namespace {
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s) {
+// Handle buffers grow stream-ordered from the device pool: no device-wide
+// synchronisation, so a handle growing its scratch never stalls work that
+// other handles have in flight.
+spgemm_status regrow(spgemm_handle_s* h, void** buf, size_t* have, size_t need,
+                     cudaStream_t stream) {
+    if (need <= *have) return SPGEMM_OK;
+    if (*buf != nullptr) {
+        B200_TRY(cudaFreeAsync(*buf, stream));
+        *buf = nullptr;
+        *have = 0;
+    }
+    B200_TRY(cudaMallocFromPoolAsync(buf, need, h->pool, stream));
+    *have = need;
+    return SPGEMM_OK;
+}
+
+spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s, cudaStream_t stream) {
     const size_t nctas = static_cast<size_t>(bin_ctas(m > 0 ? m : 1));
     const size_t mm = static_cast<size_t>(m > 0 ? m : 1);
     size_t off = 0;
@@ -141,17 +157,9 @@ spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s) {
     const size_t o_bins1 = take(sizeof(int32_t) * mm);
     const size_t o_bins2 = take(sizeof(int32_t) * mm);
     const size_t o_fail = take(sizeof(int32_t) * mm);
-    if (off > h->scratch_bytes) {
-        if (h->scratch != nullptr) {
-            B200_TRY(cudaDeviceSynchronize());
-            B200_TRY(cudaFree(h->scratch));
-            h->scratch = nullptr;
-            h->scratch_bytes = 0;
-        }
-        const size_t bytes = off + off / 4;
-        B200_TRY(cudaMalloc(&h->scratch, bytes));
-        h->scratch_bytes = bytes;
-    }
+    if (spgemm_status st = regrow(h, &h->scratch, &h->scratch_bytes, off + off / 4, stream);
+        st != SPGEMM_OK)
+        return st;
     char* b = static_cast<char*>(h->scratch);
     s->status = reinterpret_cast<DevStatus*>(b + o_status);
     s->plan1 = reinterpret_cast<Plan*>(b + o_plan1);
@@ -166,22 +174,17 @@ spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s) {
     return SPGEMM_OK;
 }
 
-spgemm_status ensure_bitmaps(spgemm_handle_s* h, int64_t words, int32_t rows, int32_t* nmaps) {
+spgemm_status ensure_bitmaps(spgemm_handle_s* h, int64_t words, int32_t rows, int32_t* nmaps,
+                            cudaStream_t stream) {
     const int64_t per_map = words * 4;
     int64_t n = std::min<int64_t>(rows, h->sm_count);
     n = std::min<int64_t>(n, std::max<int64_t>(1, kBitmapBudget / std::max<int64_t>(per_map, 1)));
     n = std::max<int64_t>(n, 1);
     const size_t need = static_cast<size_t>(n * per_map);
-    if (need > h->bitmap_bytes) {
-        if (h->bitmaps != nullptr) {
-            B200_TRY(cudaDeviceSynchronize());
-            B200_TRY(cudaFree(h->bitmaps));
-            h->bitmaps = nullptr;
-            h->bitmap_bytes = 0;
-        }
-        B200_TRY(cudaMalloc(reinterpret_cast<void**>(&h->bitmaps), need));
-        h->bitmap_bytes = need;
-    }
+    if (spgemm_status st = regrow(h, reinterpret_cast<void**>(&h->bitmaps), &h->bitmap_bytes,
+                                  need, stream);
+        st != SPGEMM_OK)
+        return st;
     *nmaps = static_cast<int32_t>(n);
     return SPGEMM_OK;
 }
@@ -344,7 +347,9 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     const BinLauncher* sym = nullptr;
     const int nsym = sym1_ladder(&sym);
     const BinLauncher* fil = nullptr;
-    const int nfil = sizeof(V) == 8 ? s2n_ladder_f64(&fil) : s2n_ladder_f32(&fil);
+    const bool narrow = n <= kBitmapCols;
+    const int nfil = sizeof(V) == 8 ? (narrow ? s2n_bitmap_ladder_f64(&fil) : s2n_ladder_f64(&fil))
+                                    : (narrow ? s2n_bitmap_ladder_f32(&fil) : s2n_ladder_f32(&fil));
     h->info.n_sym_bins = nsym;
     h->info.n_num_bins = nfil;
 
@@ -374,7 +379,7 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     } while (0)
 
     Scratch s;
-    B200_STEP(ensure_scratch(h, m, &s));
+    B200_STEP(ensure_scratch(h, m, &s, stream));
     // status, plans and fail counter are contiguous at the front of the scratch
     if (cudaError_t e = cudaMemsetAsync(
             h->scratch, 0, reinterpret_cast<char*>(s.hist1) - static_cast<char*>(h->scratch),
@@ -446,7 +451,7 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     const int32_t global_rows = p1.bin_size[glob1];
     if (cluster_rows > 0 || global_rows > 0) {
         int32_t nmaps = 0;
-        B200_STEP(ensure_bitmaps(h, pa.words, std::max(cluster_rows, global_rows), &nmaps));
+        B200_STEP(ensure_bitmaps(h, pa.words, std::max(cluster_rows, global_rows), &nmaps, stream));
         pa.bitmaps = h->bitmaps;
         pa.nmaps = nmaps;
     }
@@ -539,7 +544,7 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     pa.c_val = C->val;
     if (p2.bin_size[nfil - 1] > 0) {
         int32_t nmaps = 0;
-        B200_STEP(ensure_bitmaps(h, pa.words, p2.bin_size[nfil - 1], &nmaps));
+        B200_STEP(ensure_bitmaps(h, pa.words, p2.bin_size[nfil - 1], &nmaps, stream));
         pa.bitmaps = h->bitmaps;
         pa.nmaps = nmaps;
     }
@@ -653,7 +658,7 @@ spgemm_status batch(spgemm_handle_s* h, const spgemm_batch_desc* d, const spgemm
     h->checked = 0;  // group views start mid-matrix; the packed operands are checked once
     if (saved_checked) {
         Scratch sc;
-        if (spgemm_status st = ensure_scratch(h, std::max(A->m, B->m), &sc); st != SPGEMM_OK) {
+        if (spgemm_status st = ensure_scratch(h, std::max(A->m, B->m), &sc, stream); st != SPGEMM_OK) {
             h->checked = saved_checked;
             return unwind(st);
         }
@@ -802,16 +807,8 @@ spgemm_status product_host(spgemm_handle_s* h, const spgemm_csr_view* A,
                align_up(sizeof(V) * size_t(v->nnz), 256);
     };
     const size_t need = bytes_of(A) + bytes_of(B);
-    if (need > h->in_bytes) {
-        if (h->in_buf != nullptr) {
-            B200_TRY(cudaDeviceSynchronize());
-            B200_TRY(cudaFree(h->in_buf));
-            h->in_buf = nullptr;
-            h->in_bytes = 0;
-        }
-        B200_TRY(cudaMalloc(&h->in_buf, need));
-        h->in_bytes = need;
-    }
+    if (spgemm_status st = regrow(h, &h->in_buf, &h->in_bytes, need, stream); st != SPGEMM_OK)
+        return st;
     char* p = static_cast<char*>(h->in_buf);
     auto upload = [&](const spgemm_csr_view* v, spgemm_csr_view* d) -> cudaError_t {
         *d = *v;
@@ -872,6 +869,32 @@ spgemm_status product_host(spgemm_handle_s* h, const spgemm_csr_view* A,
     return SPGEMM_OK;
 }
 
+// One stream-ordered memory pool per device for every handle's results,
+// created on first use and never destroyed: results may outlive the handle
+// that made them, and a pool must not go away under live allocations.  Its
+// release threshold is the maximum, so freed memory stays mapped for the next
+// product (trimmed when a handle is destroyed).
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+
+spgemm_status device_pool(int dev, cudaMemPool_t* out) {
+    if (dev < 0 || dev >= 64) return fail(SPGEMM_ERR_INVALID_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (g_pools[dev] == nullptr) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        B200_TRY(cudaMemPoolCreate(&p, &props));
+        uint64_t keep = UINT64_MAX;
+        B200_TRY(cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep));
+        g_pools[dev] = p;
+    }
+    *out = g_pools[dev];
+    return SPGEMM_OK;
+}
+
 }  // namespace
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
@@ -925,13 +948,7 @@ spgemm_status spgemm_create(spgemm_handle_t* handle, int device) {
     }
     B200_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&h->mirror), sizeof(HostMirror)));
-    cudaMemPoolProps props = {};
-    props.allocType = cudaMemAllocationTypePinned;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = dev;
-    B200_TRY(cudaMemPoolCreate(&h->pool, &props));
-    uint64_t keep = UINT64_MAX;
-    B200_TRY(cudaMemPoolSetAttribute(h->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    if (spgemm_status st = device_pool(dev, &h->pool); st != SPGEMM_OK) return st;
     *handle = h;
     return SPGEMM_OK;
 }
@@ -950,8 +967,9 @@ spgemm_status spgemm_destroy(spgemm_handle_t h) {
     if (h->in_buf) cudaFree(h->in_buf);
     if (h->mirror) cudaFreeHost(h->mirror);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
-    // outstanding results keep the pool alive until they are freed
-    if (h->pool) cudaMemPoolDestroy(h->pool);
+    // the pool is shared and outlives handles (results may outlive them too);
+    // give its unused cached memory back
+    if (h->pool) cudaMemPoolTrimTo(h->pool, 0);
     delete h;
     return SPGEMM_OK;
 }
@@ -1035,7 +1053,7 @@ spgemm_status spgemm_get_nip(spgemm_handle_t h, const spgemm_csr_view* A,
     B200_TRY(cudaSetDevice(h->device));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Scratch sc;
-    if (spgemm_status st = ensure_scratch(h, A->m, &sc); st != SPGEMM_OK) return st;
+    if (spgemm_status st = ensure_scratch(h, A->m, &sc, s); st != SPGEMM_OK) return st;
     long long* d = reinterpret_cast<long long*>(sc.cta_sum);
     B200_TRY(cudaMemsetAsync(d, 0, sizeof(long long), s));
     B200_TRY(launch_total_nip(A->rpt, A->col, B->rpt, A->m, d, s));
@@ -1106,8 +1124,10 @@ spgemm_status spgemm_ladder_info(spgemm_handle_t h, int which, int dtype_bytes, 
     int nb = 0;
     if (which == 0) {
         nb = sym1_ladder(&l);
-    } else {
+    } else if (which == 1) {
         nb = dtype_bytes == 8 ? s2n_ladder_f64(&l) : s2n_ladder_f32(&l);
+    } else {
+        nb = dtype_bytes == 8 ? s2n_bitmap_ladder_f64(&l) : s2n_bitmap_ladder_f32(&l);
     }
     *n_bins = nb;
     for (int i = 0; i < 16; i++) limits[i] = i < nb ? l[i].limit : 0;

@@ -2,21 +2,27 @@
 
 Requests ``C = A * B`` (operands already on the device) arrive at any time.
 Worker threads, each owning a library handle (its own side streams, scratch and
-memory pool), repeatedly
+stream), repeatedly
 
-1. admit waiting requests, oldest first, while the outputs they may need fit
-   the memory budget: the bound is the binning phase's upper bound on C,
-   ``bytes(C) <= 4 (m + 1) + NIP * (4 + sizeof(value))`` (NIP = intermediate
-   products, computed on the device when the request is submitted);
-2. pack the admitted requests into block-diagonal operands and run them as ONE
+1. size new arrivals on the device: NIP (intermediate products) of each, in
+   small chunks so that admission starts before a burst is fully sized; the
+   binning phase's upper bound on the output,
+   ``bytes(C) <= 4 (m + 1) + NIP * (4 + sizeof(value))``, is the request's
+   share of the memory budget;
+2. admit, oldest first: a request with ``NIP >= solo_nip`` fills the GPU by
+   itself and runs alone on the plain path; smaller ones are taken in arrival
+   order (passing over large ones, which the next admission takes) while the
+   budget, ``max_batch`` and the per-batch NIP cap ``batch_nip`` allow;
+3. pack the small requests into block-diagonal operands and run them as ONE
    batched product (``spgemm_batch_*``), so rows of different requests share
    bins and kernels;
-3. hand each request its own CSR result and release its share of the budget.
+4. hand each request its own CSR result and release its share of the budget.
 
-With two workers, a batch is packed and launched while the previous one is
-still on the GPU, and requests that arrive meanwhile join the next batch: work
-from different batches overlaps on the device.  The reference has no served or
-batched form; it multiplies one pair per call (proposal.cuh:85-124).
+Large products gain nothing from packing (their rows already fill every bin),
+and a small request packed with one would wait for it, so the two kinds are
+never mixed.  With two workers a large product and a batch of small ones run
+side by side on the GPU.  The reference has no served or batched form; it
+multiplies one pair per call (proposal.cuh:85-124).
 """
 from __future__ import annotations
 
@@ -27,7 +33,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .api import DeviceCSR, Handle, PackedBatch, batch, get_nip, pack_batch
+from .api import DeviceCSR, Handle, PackedBatch, batch, get_nip, pack_batch, proposal
 
 
 @dataclass
@@ -40,6 +46,7 @@ class Request:
     t_done: float = 0.0
     bound_bytes: int = 0
     nip: int = 0
+    sizing: bool = False
     result: DeviceCSR | None = None
     error: BaseException | None = None
     done: threading.Event = field(default_factory=threading.Event)
@@ -55,41 +62,47 @@ class SpgemmServer:
     memory_budget: bytes of C bounds that may be in flight at once.
     max_batch:     most requests packed into one batched product.
     workers:       worker threads (handles); 2 lets batches overlap.
+    solo_nip:      requests with at least this many intermediate products run
+                   alone on the plain path.
+    batch_nip:     cap on the intermediate products of one batch (bounds the
+                   time a batch's first request waits for its last).
+    size_chunk:    arrivals a worker sizes before it tries to admit.
     """
 
     def __init__(self, memory_budget: int = 32 << 30, max_batch: int = 256, workers: int = 2,
-                 device: int = 0):
+                 device: int = 0, solo_nip: int = 4 << 20, batch_nip: int = 32 << 20,
+                 size_chunk: int = 16):
         import torch
         self._torch = torch
         self.device = device
         self.memory_budget = int(memory_budget)
         self.max_batch = int(max_batch)
+        self.solo_nip = int(solo_nip)
+        self.batch_nip = int(batch_nip)
+        self.size_chunk = int(size_chunk)
         self._queue: deque[Request] = deque()
         self._cv = threading.Condition()
         self._in_flight_bytes = 0
         self._stop = False
         self._handles = [Handle(device) for _ in range(workers)]
-        self._sizer = Handle(device)
-        self._sizer_lock = threading.Lock()
         self._next_id = 0
         self.batches = 0
         self.batched_requests = 0
-        self._threads = [threading.Thread(target=self._worker, args=(h,), daemon=True)
-                         for h in self._handles]
+        # per batch: (worker, requests, t_admitted, t_launched, t_done), perf_counter s
+        self.timeline: list[tuple[int, int, float, float, float]] = []
+        self._threads = [threading.Thread(target=self._worker, args=(i, h), daemon=True)
+                         for i, h in enumerate(self._handles)]
         for t in self._threads:
             t.start()
 
     # -- client side --------------------------------------------------------
     def submit(self, A: DeviceCSR, B: DeviceCSR, t_arrival: float | None = None) -> Request:
-        """Queue C = A * B.  Computes the request's NIP on the device (its
-        admission bound) and returns the Request; wait on req.done."""
+        """Queue C = A * B and return the Request; wait on req.done.  The
+        request's admission bound is computed by a worker, on the device."""
         if A.n != B.m:
             raise ValueError("A.n must equal B.m")
-        with self._sizer_lock:
-            nip = get_nip(A, B, self._sizer)
-        s = A.val.element_size()
         req = Request(A, B, t_arrival=time.perf_counter() if t_arrival is None else t_arrival,
-                      nip=nip, bound_bytes=4 * (A.m + 1) + nip * (4 + s))
+                      bound_bytes=-1)
         with self._cv:
             req.rid = self._next_id
             self._next_id += 1
@@ -105,26 +118,46 @@ class SpgemmServer:
             t.join()
         for h in self._handles:
             h.close()
-        self._sizer.close()
 
     # -- worker side --------------------------------------------------------
-    def _admit(self) -> list[Request]:
-        """Oldest-first admission under the memory budget (call with the lock
-        held).  A request larger than the whole budget runs alone."""
+    def _admit(self) -> tuple[list[Request], bool]:
+        """Take the next unit of work (call with the lock held): a large
+        request alone (second value True), or small requests in arrival order
+        under the budget, max_batch and batch_nip.  Unsized requests stop the
+        scan, so admission order is arrival order.  A request larger than the
+        whole budget runs when nothing else is in flight."""
         taken: list[Request] = []
+        nip = 0
+        skipped = []
         while self._queue and len(taken) < self.max_batch:
             r = self._queue[0]
+            if r.bound_bytes < 0:
+                break
             fits = self._in_flight_bytes + r.bound_bytes <= self.memory_budget
+            if r.nip >= self.solo_nip:
+                if taken:  # leave it for the next admission
+                    skipped.append(self._queue.popleft())
+                    continue
+                if not fits and self._in_flight_bytes > 0:
+                    break
+                self._queue.popleft()
+                self._in_flight_bytes += r.bound_bytes
+                self._queue.extendleft(reversed(skipped))
+                return [r], True
             if not fits and (taken or self._in_flight_bytes > 0):
+                break
+            if taken and nip + r.nip > self.batch_nip:
                 break
             self._queue.popleft()
             self._in_flight_bytes += r.bound_bytes
+            nip += r.nip
             taken.append(r)
             if not fits:
                 break
-        return taken
+        self._queue.extendleft(reversed(skipped))
+        return taken, False
 
-    def _worker(self, handle: Handle) -> None:
+    def _worker(self, wid: int, handle: Handle) -> None:
         torch = self._torch
         torch.cuda.set_device(self.device)
         stream = torch.cuda.Stream(device=self.device)
@@ -134,23 +167,47 @@ class SpgemmServer:
                     self._cv.wait()
                 if self._stop and not self._queue:
                     return
-                reqs = self._admit()
+                unsized = []
+                for r in self._queue:
+                    if r.bound_bytes < 0 and not r.sizing:
+                        r.sizing = True
+                        unsized.append(r)
+                        if len(unsized) == self.size_chunk:
+                            break
+            if unsized:
+                # admission bounds of new arrivals, on this worker's stream
+                for r in unsized:
+                    try:
+                        r.nip = get_nip(r.A, r.B, handle, stream)
+                    except BaseException as e:
+                        r.error = e
+                        r.nip = 0
+                    r.bound_bytes = 4 * (r.A.m + 1) + r.nip * (4 + r.A.val.element_size())
+                with self._cv:
+                    self._cv.notify_all()
+            with self._cv:
+                reqs, solo = self._admit()
                 if not reqs:
-                    self._cv.wait(timeout=0.001)
+                    if not unsized:
+                        self._cv.wait(timeout=0.0005)
                     continue
             now = time.perf_counter()
             for r in reqs:
                 r.t_admitted = now
+            failed = [r for r in reqs if r.error is not None]
+            reqs = [r for r in reqs if r.error is None]
+            t_launch = now
             try:
                 with torch.cuda.stream(stream):
-                    if len(reqs) == 1:
-                        pb = PackedBatch(np.array([0, reqs[0].A.m], np.int32),
-                                         np.array([0, reqs[0].B.m], np.int32),
-                                         np.array([0, reqs[0].B.n], np.int32),
-                                         reqs[0].A, reqs[0].B)
+                    if not reqs:
+                        outs = []
+                    elif solo or len(reqs) == 1:
+                        t_launch = time.perf_counter()
+                        outs = [proposal(reqs[0].A, reqs[0].B, handle, stream)]
                     else:
                         pb = pack_batch([(r.A, r.B) for r in reqs])
-                    outs = batch(pb, handle, stream)
+                        t_launch = time.perf_counter()
+                        outs = batch(pb, handle, stream)
                     stream.synchronize()
                 done = time.perf_counter()
                 for r, c in zip(reqs, outs):
@@ -161,6 +218,10 @@ class SpgemmServer:
                 for r in reqs:
                     r.error = e
                     r.t_done = done
+            for r in failed:
+                r.t_done = done
+            reqs += failed
+            self.timeline.append((wid, len(reqs), now, t_launch, done))
             with self._cv:
                 self._in_flight_bytes -= sum(r.bound_bytes for r in reqs)
                 self.batches += 1

@@ -189,8 +189,10 @@ SPGEMM_API spgemm_status spgemm_last_profile(spgemm_handle_t handle, spgemm_kern
                                              int32_t capacity, int32_t* count);
 
 /* Number of bins of each ladder and the key limit of bin `bin` (rows whose
- * key -- NIP for the count ladder, nnz for the fill ladder -- is <= limit). */
-SPGEMM_API spgemm_status spgemm_ladder_info(spgemm_handle_t handle, int which /*0 sym, 1 num*/,
+ * key -- NIP for the count ladder, nnz for the fill ladders -- is <= limit).
+ * which: 0 count ladder; 1 fill ladder used when B.n > 2^20; 2 fill ladder
+ * used when B.n <= 2^20 (its large rows use a shared-memory bitmap). */
+SPGEMM_API spgemm_status spgemm_ladder_info(spgemm_handle_t handle, int which,
                                  int dtype_bytes, int* n_bins, int64_t* limits /*[16]*/);
 
 /* ---- batched products ------------------------------------------------------ */

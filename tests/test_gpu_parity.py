@@ -103,19 +103,73 @@ def test_forced_sym_bin(handle, oracle_mod, b):
     check(oracle_mod, A, A, C, np.float64, f"forced_sym_bin{b}", positive=True)
 
 
+def _wide_pair():
+    """B with more than 2^20 columns: the fill ladder with hash CTA bins."""
+    A = G.power_law(3000, 2.0, 300, seed=43)
+    B = G.uniform_rows((1 << 20) + 5, 8, seed=44, m=3000)
+    return A, B
+
+
 @pytest.mark.parametrize("b", range(9))
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
-def test_forced_num_bin(handle, oracle_mod, b, dtype):
+@pytest.mark.parametrize("width", ["narrow", "wide"])
+def test_forced_num_bin(handle, oracle_mod, b, dtype, width):
     from gpuspgemm_b200 import _native as N
-    if b >= _ladder_len(handle, 1):
+    which = 2 if width == "narrow" else 1
+    if b >= len(handle.ladder(which, 8)):
         pytest.skip("no such bin")
-    A = G.power_law(3000, 2.0, 300, seed=42)
+    if width == "narrow":
+        A = G.power_law(3000, 2.0, 300, seed=42)
+        B = A
+    else:
+        A, B = _wide_pair()
     handle.set_option(N.OPT_MIN_NUM_BIN, b)
     try:
-        C = gpu_product(A, A, handle, dtype)
+        C = gpu_product(A, B, handle, dtype)
     finally:
         handle.set_option(N.OPT_MIN_NUM_BIN, -1)
-    check(oracle_mod, A, A, C, dtype, f"forced_num_bin{b}", positive=True)
+    check(oracle_mod, A, B, C, dtype, f"forced_num_bin{b}_{width}", positive=True)
+
+
+@pytest.mark.parametrize("shuffle", [False, True])
+def test_global_bins_block_diagonal(handle, oracle_mod, shuffle):
+    """Every row in the global bitmap bins of both phases, on a block-diagonal
+    product (each row's column window is one block).  With `shuffle`, rows of B
+    are unsorted, so keys fall outside the first/last-column window and the
+    kernels redo those rows over all of B's columns."""
+    from gpuspgemm_b200 import _native as N
+    blocks = [G.power_law(1500, 2.0, 300, seed=900 + i) for i in range(3)]
+    A = _block_diag(blocks)
+    B = HostCSR(A.m, A.n, A.rpt.copy(), A.col.copy(), A.val.copy())
+    if shuffle:
+        rng = np.random.default_rng(5)
+        for r in range(0, B.m, 7):
+            s, e = B.rpt[r], B.rpt[r + 1]
+            p = rng.permutation(e - s)
+            B.col[s:e] = B.col[s:e][p]
+            B.val[s:e] = B.val[s:e][p]
+    handle.set_option(N.OPT_MIN_SYM_BIN, _ladder_len(handle, 0) - 1)
+    handle.set_option(N.OPT_MIN_NUM_BIN, _ladder_len(handle, 2) - 1)
+    try:
+        C = gpu_product(A, B, handle, np.float64)
+    finally:
+        handle.set_option(N.OPT_MIN_SYM_BIN, -1)
+        handle.set_option(N.OPT_MIN_NUM_BIN, -1)
+    check(oracle_mod, A, A, C, np.float64, f"global_blockdiag_shuffle{int(shuffle)}",
+          positive=True)
+
+
+def _block_diag(mats):
+    rpt, cols, vals = [np.zeros(1, np.int32)], [], []
+    nz = c0 = 0
+    for M in mats:
+        rpt.append(M.rpt[1:] + nz)
+        cols.append(M.col + c0)
+        vals.append(M.val)
+        nz += M.nnz
+        c0 += M.n
+    return HostCSR(sum(M.m for M in mats), c0, np.concatenate(rpt).astype(np.int32),
+                   np.concatenate(cols).astype(np.int32), np.concatenate(vals))
 
 
 def test_heavy_row_spills_to_global(handle, oracle_mod):
