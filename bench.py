@@ -53,9 +53,12 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--out", type=str, default="")
-    ap.add_argument("--mode", choices=["plain", "batch", "served"], default="plain",
+    ap.add_argument("--mode", choices=["plain", "batch", "served", "galerkin"], default="plain",
                     help="plain: the headline C=A*A workload; batch: many independent "
-                         "products (batched form vs one call per product)")
+                         "products (batched form vs one call per product); served: a "
+                         "request stream; galerkin: R*A*P on a 27-point stencil")
+    ap.add_argument("--grid", type=int, default=100,
+                    help="galerkin mode: points per dimension of the 27-point stencil")
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--requests", type=int, default=600)
     ap.add_argument("--load", type=float, default=0.8,
@@ -453,6 +456,114 @@ def run_batch(args, local_rank):
     }
 
 
+# ---- Galerkin triple product: R * (A * P) on a 27-point stencil ------------------
+
+def run_galerkin(args, local_rank):
+    import torch
+
+    from gpuspgemm_b200 import generators as G
+    from gpuspgemm_b200.api import DeviceCSR, Handle, get_nip, proposal, rap, transpose
+
+    torch.cuda.set_device(local_rank)
+    npdt = np.float32 if args.dtype == "f32" else np.float64
+    A_h = G.stencil27(args.grid).astype(npdt)
+    P_h = G.aggregation_prolongator(args.grid, seed=args.seed).astype(npdt)
+    A, P = DeviceCSR.from_host(A_h), DeviceCSR.from_host(P_h)
+    h = Handle(local_rank)
+    stream = torch.cuda.current_stream()
+    for _ in range(max(args.warmup, 3)):
+        C = rap(A, P, None, h)
+        del C
+    R = transpose(P, h)
+    AP = proposal(A, P, h)
+    nip_ap = get_nip(A, P, h)
+    nip_rap = get_nip(R, AP, h)
+    C = proposal(R, AP, h)
+    nnz_ap, nnz_c = AP.nnz, C.nnz
+    del AP, C
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    # the chain as one call (inputs of 300+ MB: larger than L2), and its stages
+    t_call, t_tr, t_ap, t_rap = [], [], [], []
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            e = [ev() for _ in range(5)]
+            e[0].record(stream)
+            C = rap(A, P, None, h)
+            e[1].record(stream)
+            del C
+            Rt = transpose(P, h)
+            e[2].record(stream)
+            AP = proposal(A, P, h)
+            e[3].record(stream)
+            C = proposal(Rt, AP, h)
+            e[4].record(stream)
+            torch.cuda.synchronize()
+            t_call.append(e[0].elapsed_time(e[1]))
+            t_tr.append(e[1].elapsed_time(e[2]))
+            t_ap.append(e[2].elapsed_time(e[3]))
+            t_rap.append(e[3].elapsed_time(e[4]))
+            del C, AP, Rt
+    ms = float(np.mean(t_call))
+    flops = 2.0 * (nip_ap + nip_rap)
+    # end to end: operands from pinned host memory, C back to the host
+    pin = [torch.from_numpy(np.ascontiguousarray(x)).pin_memory()
+           for x in (A_h.rpt, A_h.col, A_h.val, P_h.rpt, P_h.col, P_h.val)]
+    h2d = sum(t.numel() * t.element_size() for t in pin)
+    e2e = []
+    d2h = 0
+    for _ in range(max(1, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        d = [t.to("cuda", non_blocking=True) for t in pin]
+        C = rap(DeviceCSR(A_h.m, A_h.n, d[0], d[1], d[2]), DeviceCSR(P_h.m, P_h.n, d[3], d[4], d[5]),
+                None, h)
+        out = [x.to("cpu") for x in (C.rpt, C.col, C.val)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e.append(e0.elapsed_time(e1))
+        d2h = sum(t.numel() * t.element_size() for t in out)
+        del C, d, out
+    e2e_ms = float(np.mean(e2e))
+    line = {
+        "metric": "Galerkin product R*(A*P) GFLOPS (2*NIP/s over both products)",
+        "value": flops / (ms / 1e3) / 1e9, "unit": "GFLOPS", "n_gpus": 1,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": args.dtype, "data": "synthetic (seeded generator)",
+        "config": {"workload": f"27-point stencil on {args.grid}^3, aggregation prolongator "
+                               f"3^3 blocks with smoothed fill (<= 8 nnz/row), R = P^T on the "
+                               "device", "A": [A_h.m, A_h.n, A_h.nnz], "P": [P_h.m, P_h.n, P_h.nnz],
+                   "nip_AP": nip_ap, "nnz_AP": nnz_ap, "nip_RAP": nip_rap, "nnz_C": nnz_c,
+                   "l2": "operands larger than L2 (A alone is "
+                         f"{(A_h.nnz * (4 + A_h.val.itemsize)) >> 20} MB)"},
+        "stages_ms": {"transpose_P": float(np.mean(t_tr)), "A_times_P": float(np.mean(t_ap)),
+                      "R_times_AP": float(np.mean(t_rap))},
+        "e2e": {"value": flops / (e2e_ms / 1e3) / 1e9, "unit": "GFLOPS",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "ms_per_step": e2e_ms},
+        "clocks": clk.summary(),
+    }
+    h.close()
+    if not args.no_cpu_baseline:
+        import time as _t
+
+        import oracle
+        cores = oracle.max_threads()
+        t0 = _t.perf_counter()
+        AP_c = oracle.spgemm(A_h, P_h)
+        oracle.spgemm(oracle.transpose(P_h), AP_c)
+        dt = _t.perf_counter() - t0
+        line["cpu_baseline"] = {"value": flops / dt / 1e9, "unit": "GFLOPS", "cores": cores,
+                                "kind": "port", "sample": "the full chain once (row-wise "
+                                "Gustavson, OpenMP; numpy transpose)"}
+    return line
+
+
 # ---- served form: Poisson arrivals of mixed-size requests ----------------------
 
 def served_pool(seed: int):
@@ -598,6 +709,8 @@ def main():
         line = run_batch(args, local_rank) if rank == 0 else None
     elif args.mode == "served":
         line = run_served(args, local_rank) if rank == 0 else None
+    elif args.mode == "galerkin":
+        line = run_galerkin(args, local_rank) if rank == 0 else None
     elif args.impl == "reference":
         line = run_reference(args, rank)
     else:

@@ -28,6 +28,7 @@ OPT_MIN_NUM_BIN = 3
 OPT_CLUSTER_SIZE = 4
 OPT_STREAMS = 5
 OPT_PROFILE = 6
+OPT_MIN_TRANSPOSE_BIN = 7
 
 
 class CsrView(C.Structure):
@@ -125,6 +126,14 @@ SIGNATURES = {
     "spgemm_batch_f32": (C.c_int, [C.c_void_p, C.POINTER(BatchDesc), C.POINTER(CsrView),
                                    C.POINTER(CsrView), C.POINTER(BatchOut), C.c_void_p]),
     "spgemm_batch_free": (C.c_int, [C.POINTER(BatchOut), C.c_void_p]),
+    "spgemm_transpose_f64": (C.c_int, [C.c_void_p, C.POINTER(CsrView), C.POINTER(CsrOut),
+                                       C.c_void_p]),
+    "spgemm_transpose_f32": (C.c_int, [C.c_void_p, C.POINTER(CsrView), C.POINTER(CsrOut),
+                                       C.c_void_p]),
+    "spgemm_rap_f64": (C.c_int, [C.c_void_p, C.POINTER(CsrView), C.POINTER(CsrView),
+                                 C.POINTER(CsrView), C.POINTER(CsrOut), C.c_void_p]),
+    "spgemm_rap_f32": (C.c_int, [C.c_void_p, C.POINTER(CsrView), C.POINTER(CsrView),
+                                 C.POINTER(CsrView), C.POINTER(CsrOut), C.c_void_p]),
     "spgemm_row_nnz_noalloc": (C.c_int, [C.POINTER(CsrView), C.POINTER(CsrView), C.c_void_p,
                                          C.c_void_p]),
     "spgemm_last_error_string": (C.c_char_p, []),

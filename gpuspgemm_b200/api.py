@@ -393,6 +393,37 @@ def proposal_host(A: HostCSR, B: HostCSR, handle: Handle | None = None,
     return HostCSR(m, n, rpt, col, val)
 
 
+def transpose(A: DeviceCSR, handle: Handle | None = None, stream=None) -> DeviceCSR:
+    """A^T on the device, columns sorted (spgemm_transpose_*).  The reference
+    has no transpose; its Galerkin use forms R = P^T outside the library."""
+    _require_torch()
+    h = handle or default_handle()
+    out = N.CsrOut()
+    va = A.view()
+    fn = N.lib().spgemm_transpose_f64 if A.dtype == torch.float64 else \
+        N.lib().spgemm_transpose_f32
+    N.check(fn(h.ptr, C.byref(va), C.byref(out), _stream_ptr(stream)))
+    return _wrap_result(out, A.dtype)
+
+
+def rap(A: DeviceCSR, P: DeviceCSR, R: DeviceCSR | None = None, handle: Handle | None = None,
+        stream=None) -> DeviceCSR:
+    """Galerkin triple product C = R * (A * P) (spgemm_rap_*); R = None means
+    R = P^T, transposed on the device.  Replaces two proposal calls
+    (proposal.cuh:85-124) plus a caller-side transpose."""
+    _require_torch()
+    if A.dtype != P.dtype or (R is not None and R.dtype != A.dtype):
+        raise TypeError("R, A and P must have the same value dtype")
+    h = handle or default_handle()
+    out = N.CsrOut()
+    va, vp = A.view(), P.view()
+    vr = R.view() if R is not None else None
+    fn = N.lib().spgemm_rap_f64 if A.dtype == torch.float64 else N.lib().spgemm_rap_f32
+    N.check(fn(h.ptr, C.byref(vr) if vr is not None else None, C.byref(va), C.byref(vp),
+               C.byref(out), _stream_ptr(stream)))
+    return _wrap_result(out, A.dtype)
+
+
 def get_nip(A: DeviceCSR, B: DeviceCSR, handle: Handle | None = None, stream=None) -> int:
     """Total intermediate products (reference utils::get_nip, nip.cuh:52-78)."""
     h = handle or default_handle()

@@ -26,7 +26,8 @@ LIB = PKG / "libspgemm_b200.so"
 # build time with USE_DOUBLE_PRECISION, cmake/options.cmake:2-3)
 APPS = {PKG / "spgemm_app": ["-DUSE_DOUBLE_PRECISION"], PKG / "spgemm_app_f32": []}
 
-SOURCES = ["k_bin.cu", "k_sym1.cu", "k_s2n.cu", "k_batch.cu", "spgemm.cu", "noalloc.cu"]
+SOURCES = ["k_bin.cu", "k_sym1.cu", "k_s2n.cu", "k_batch.cu", "k_transpose.cu", "spgemm.cu",
+           "noalloc.cu"]
 APP_SOURCES = ["app/spgemm_app.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -55,6 +55,8 @@ struct ProductArgs {
     int32_t cluster;        // CTAs per cluster
     int32_t* fail_rows;     // rows that spilled out of a cluster table
     int32_t* fail_count;
+    // transpose: per entry of T, (row of A << 32 | position in A)
+    uint64_t* keys;
 };
 
 enum class BinKind : int { Team = 0, Cta = 1, Cluster = 2, Global = 3 };
@@ -115,6 +117,16 @@ cudaError_t launch_product_nip(const int32_t* a_rpt, const int32_t* a_col, const
 cudaError_t launch_unpack(const int32_t* c_rpt, int32_t* c_col, const int32_t* row_off,
                           const int32_t* col_off, const int64_t* out_off, int32_t first,
                           int32_t count, int32_t* rpt_out, int32_t* pos_out, cudaStream_t s);
+// CSR transpose (k_transpose.cu): row-sort ladder (key = length of a row of
+// A^T), column counts, and the keyed scatter.
+int transpose_ladder_f64(const BinLauncher** out);
+int transpose_ladder_f32(const BinLauncher** out);
+cudaError_t transpose_prepare();
+cudaError_t launch_col_count(const int32_t* col, int32_t nnz, int32_t n, int32_t* cnt,
+                             cudaStream_t s);
+cudaError_t launch_tr_scatter(const int32_t* a_rpt, const int32_t* a_col, int32_t m, int32_t n,
+                              const int32_t* t_rpt, int32_t* cursor, uint64_t* keys,
+                              cudaStream_t s);
 // Total NIP only (spgemm_get_nip).
 cudaError_t launch_total_nip(const int32_t* a_rpt, const int32_t* a_col, const int32_t* b_rpt,
                              int32_t m, long long* out, cudaStream_t s);

@@ -106,6 +106,7 @@ struct spgemm_handle_s {
     int min_num_bin = -1;
     int cluster = 4;
     int profile = 0;
+    int min_tr_bin = -1;
     // C's arrays come from the device's shared stream-ordered pool (see
     // device_pool); it keeps freed memory mapped so repeated products do not
     // re-map hundreds of MB per call.  cudaFree / cudaFreeAsync release them.
@@ -869,6 +870,198 @@ spgemm_status product_host(spgemm_handle_s* h, const spgemm_csr_view* A,
     return SPGEMM_OK;
 }
 
+// ---- CSR transpose -----------------------------------------------------------
+// T = A^T with sorted columns (k_transpose.cu): column counts, the binning pass
+// with the scan (T.rpt and length bins of T's rows), a keyed scatter, then one
+// sort kernel per non-empty length bin.  One host synchronisation (the bin
+// sizes), like each binning pass of a product.
+template<typename V>
+spgemm_status transpose(spgemm_handle_s* h, const spgemm_csr_view* A, spgemm_csr_out* T,
+                        cudaStream_t stream) {
+    if (h == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "handle is NULL");
+    if (T == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "T is NULL");
+    if (spgemm_status st = check_view(A, "A"); st != SPGEMM_OK) return st;
+    std::memset(T, 0, sizeof(*T));
+    h->info = spgemm_info{};
+    h->prof.clear();
+    h->prof_done.clear();
+    B200_TRY(cudaSetDevice(h->device));
+    const int32_t m = A->m;
+    const int32_t n = A->n;
+    const int32_t nnz = A->nnz;
+    T->m = n;
+    T->n = m;
+    const BinLauncher* tl = nullptr;
+    const int ntl = sizeof(V) == 8 ? transpose_ladder_f64(&tl) : transpose_ladder_f32(&tl);
+    h->info.n_num_bins = ntl;
+    B200_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&T->rpt),
+                                     sizeof(int32_t) * (size_t(n) + 1), h->pool, stream));
+    uint64_t* keys = nullptr;
+    int32_t* cursor = nullptr;
+    auto bail = [&](spgemm_status st) {
+        const std::string msg = g_last_error;
+        cudaStreamSynchronize(stream);
+        if (keys) cudaFreeAsync(keys, stream);
+        if (cursor) cudaFreeAsync(cursor, stream);
+        spgemm_csr_free(T, stream);
+        cudaStreamSynchronize(stream);
+        h->prof.clear();
+        g_last_error = msg;
+        return st;
+    };
+#define B200_STEP(expr)                                                  \
+    do {                                                                 \
+        spgemm_status st_ = (expr);                                      \
+        if (st_ != SPGEMM_OK) return bail(st_);                          \
+    } while (0)
+#define B200_CUDA(expr, what)                                            \
+    do {                                                                 \
+        cudaError_t e_ = (expr);                                         \
+        if (e_ != cudaSuccess) return bail(cuda_fail(e_, what));         \
+    } while (0)
+    Scratch s;
+    B200_STEP(ensure_scratch(h, n, &s, stream));
+    B200_CUDA(cudaMemsetAsync(h->scratch, 0,
+                              reinterpret_cast<char*>(s.hist1) - static_cast<char*>(h->scratch),
+                              stream),
+              "memset scratch");
+    if (h->checked) {
+        B200_STEP(timed(h, "check_csr_A", 0, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_check_csr(A->rpt, A->col, m, n, nnz, s.status, ss);
+        }));
+        B200_STEP(sync_mirror(h, stream, s.plan1, s));
+        B200_STEP(status_to_error(h->mirror->status));
+    }
+    B200_CUDA(cudaMemsetAsync(T->rpt, 0, sizeof(int32_t) * (size_t(n) + 1), stream),
+              "memset T.rpt");
+    if (nnz == 0 || n == 0) {
+        B200_CUDA(cudaStreamSynchronize(stream), "synchronize");
+        return SPGEMM_OK;
+    }
+    B200_STEP(timed(h, "col_count", 1, -1, nnz, stream, [&](cudaStream_t ss) {
+        return launch_col_count(A->col, nnz, n, T->rpt, ss);
+    }));
+    const Ladder lad = make_ladder(tl, ntl, h->min_tr_bin);
+    const int nctas = bin_ctas(n);
+    B200_STEP(timed(h, "tr_hist", 2, -1, n, stream, [&](cudaStream_t ss) {
+        return launch_nnz_hist(T->rpt, n, s.hist2, s.cta_sum, s.plan2, lad, ss);
+    }));
+    B200_STEP(timed(h, "tr_offsets", 2, -1, n, stream, [&](cudaStream_t ss) {
+        return launch_bin_offsets(s.hist2, nctas, s.cta_sum, s.plan2, lad, ss);
+    }));
+    B200_STEP(timed(h, "tr_scan_scatter", 2, -1, n, stream, [&](cudaStream_t ss) {
+        return launch_bin_scatter(T->rpt, n, s.hist2, s.cta_sum, s.bins2, s.plan2, lad, true,
+                                  ss);
+    }));
+    B200_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&keys),
+                                      sizeof(uint64_t) * size_t(nnz), h->pool, stream),
+              "allocate transpose keys");
+    B200_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&cursor),
+                                      sizeof(int32_t) * size_t(n), h->pool, stream),
+              "allocate transpose cursors");
+    B200_CUDA(cudaMemsetAsync(cursor, 0, sizeof(int32_t) * size_t(n), stream), "memset cursors");
+    B200_STEP(timed(h, "tr_scatter", 3, -1, m, stream, [&](cudaStream_t ss) {
+        return launch_tr_scatter(A->rpt, A->col, m, n, T->rpt, cursor, keys, ss);
+    }));
+    B200_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&T->col),
+                                      sizeof(int32_t) * size_t(nnz) + 16, h->pool, stream),
+              "allocate T.col");
+    B200_CUDA(cudaMallocFromPoolAsync(&T->val, sizeof(V) * size_t(nnz), h->pool, stream),
+              "allocate T.val");
+    T->nnz = nnz;
+    B200_STEP(sync_mirror(h, stream, s.plan2, s));
+    B200_STEP(status_to_error(h->mirror->status));
+    const Plan plan = h->mirror->plan;
+    if (plan.total_key != nnz)
+        return bail(fail(SPGEMM_ERR_INVALID_ARG, "A.col holds a column index outside [0, A.n)"));
+    h->info.nnz = nnz;
+    h->info.max_row_nnz = plan.max_key;
+    for (int b = 0; b < ntl && b < 16; b++) h->info.num_bin_rows[b] = plan.bin_size[b];
+    ProductArgs pa = {};
+    pa.a_val = A->val;
+    pa.c_rpt = T->rpt;
+    pa.c_col = T->col;
+    pa.c_val = T->val;
+    pa.status = s.status;
+    pa.keys = keys;
+    B200_STEP(launch_bins(h, tl, ntl, 4, plan, s.bins2, pa, stream));
+    B200_CUDA(cudaFreeAsync(keys, stream), "free transpose keys");
+    keys = nullptr;
+    B200_CUDA(cudaFreeAsync(cursor, stream), "free transpose cursors");
+    cursor = nullptr;
+    B200_CUDA(cudaMemcpyAsync(&h->mirror->status, s.status, sizeof(DevStatus),
+                              cudaMemcpyDeviceToHost, stream),
+              "read status");
+    B200_CUDA(cudaStreamSynchronize(stream), "final synchronize");
+    h->info.host_syncs++;
+    B200_STEP(status_to_error(h->mirror->status));
+    resolve_profile(h);
+#undef B200_CUDA
+#undef B200_STEP
+    return SPGEMM_OK;
+}
+
+spgemm_csr_view view_of(const spgemm_csr_out& c) {
+    spgemm_csr_view v;
+    v.m = c.m;
+    v.n = c.n;
+    v.nnz = c.nnz;
+    v.rpt = c.rpt;
+    v.col = c.col;
+    v.val = c.val;
+    return v;
+}
+
+// ---- Galerkin triple product C = R * (A * P) -----------------------------------
+// Two chained products on the handle's scratch and pool; with R = NULL the
+// restriction is P^T, transposed on the device.  The intermediate A*P (and
+// P^T) are freed stream-ordered before return.
+template<typename V>
+spgemm_status rap(spgemm_handle_s* h, const spgemm_csr_view* R, const spgemm_csr_view* A,
+                  const spgemm_csr_view* P, spgemm_csr_out* C, cudaStream_t stream) {
+    if (h == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "handle is NULL");
+    if (C == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "C is NULL");
+    if (spgemm_status st = check_view(A, "A"); st != SPGEMM_OK) return st;
+    if (spgemm_status st = check_view(P, "P"); st != SPGEMM_OK) return st;
+    if (R != nullptr) {
+        if (spgemm_status st = check_view(R, "R"); st != SPGEMM_OK) return st;
+        if (R->n != A->m)
+            return fail(SPGEMM_ERR_INVALID_ARG, "R.n (" + std::to_string(R->n) +
+                                                    ") must equal A.m (" + std::to_string(A->m) +
+                                                    ")");
+    } else if (P->m != A->m) {
+        return fail(SPGEMM_ERR_INVALID_ARG, "with R = P^T, P.m (" + std::to_string(P->m) +
+                                                ") must equal A.m (" + std::to_string(A->m) + ")");
+    }
+    if (A->n != P->m)
+        return fail(SPGEMM_ERR_INVALID_ARG, "A.n (" + std::to_string(A->n) +
+                                                ") must equal P.m (" + std::to_string(P->m) + ")");
+    std::memset(C, 0, sizeof(*C));
+    spgemm_csr_out AP, PT;
+    std::memset(&PT, 0, sizeof(PT));
+    if (spgemm_status st = product<V>(h, A, P, &AP, stream); st != SPGEMM_OK) return st;
+    const spgemm_info info_ap = h->info;
+    spgemm_csr_view rv;
+    if (R == nullptr) {
+        if (spgemm_status st = transpose<V>(h, P, &PT, stream); st != SPGEMM_OK) {
+            spgemm_csr_free(&AP, stream);
+            return st;
+        }
+        rv = view_of(PT);
+    } else {
+        rv = *R;
+    }
+    const spgemm_csr_view apv = view_of(AP);
+    const spgemm_status st = product<V>(h, &rv, &apv, C, stream);
+    spgemm_csr_free(&AP, stream);
+    if (R == nullptr) spgemm_csr_free(&PT, stream);
+    if (st != SPGEMM_OK) return st;
+    // info describes the second product; NIP and host syncs cover the chain
+    h->info.nip += info_ap.nip;
+    h->info.host_syncs += info_ap.host_syncs;
+    return SPGEMM_OK;
+}
+
 // One stream-ordered memory pool per device for every handle's results,
 // created on first use and never destroyed: results may outlive the handle
 // that made them, and a pool must not go away under live allocations.  Its
@@ -942,6 +1135,7 @@ spgemm_status spgemm_create(spgemm_handle_t* handle, int device) {
     B200_TRY(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, dev));
     B200_TRY(sym1_prepare());
     B200_TRY(s2n_prepare());
+    B200_TRY(transpose_prepare());
     for (int i = 0; i < kMaxSide; i++) {
         B200_TRY(cudaStreamCreateWithFlags(&h->side[i], cudaStreamNonBlocking));
         B200_TRY(cudaEventCreateWithFlags(&h->ev_join[i], cudaEventDisableTiming));
@@ -992,6 +1186,28 @@ spgemm_status spgemm_csr_host_f64(spgemm_handle_t h, const spgemm_csr_view* A,
 spgemm_status spgemm_csr_host_f32(spgemm_handle_t h, const spgemm_csr_view* A,
                                   const spgemm_csr_view* B, spgemm_csr_out* C, void* stream) {
     return product_host<float>(h, A, B, C, static_cast<cudaStream_t>(stream));
+}
+
+spgemm_status spgemm_transpose_f64(spgemm_handle_t h, const spgemm_csr_view* A,
+                                   spgemm_csr_out* T, void* stream) {
+    return transpose<double>(h, A, T, static_cast<cudaStream_t>(stream));
+}
+
+spgemm_status spgemm_transpose_f32(spgemm_handle_t h, const spgemm_csr_view* A,
+                                   spgemm_csr_out* T, void* stream) {
+    return transpose<float>(h, A, T, static_cast<cudaStream_t>(stream));
+}
+
+spgemm_status spgemm_rap_f64(spgemm_handle_t h, const spgemm_csr_view* R,
+                             const spgemm_csr_view* A, const spgemm_csr_view* P,
+                             spgemm_csr_out* C, void* stream) {
+    return rap<double>(h, R, A, P, C, static_cast<cudaStream_t>(stream));
+}
+
+spgemm_status spgemm_rap_f32(spgemm_handle_t h, const spgemm_csr_view* R,
+                             const spgemm_csr_view* A, const spgemm_csr_view* P,
+                             spgemm_csr_out* C, void* stream) {
+    return rap<float>(h, R, A, P, C, static_cast<cudaStream_t>(stream));
 }
 
 spgemm_status spgemm_batch_f64(spgemm_handle_t h, const spgemm_batch_desc* d,
@@ -1099,6 +1315,7 @@ spgemm_status spgemm_set_option(spgemm_handle_t h, spgemm_option opt, int64_t va
             h->nside = static_cast<int>(value);
             return SPGEMM_OK;
         case SPGEMM_OPT_PROFILE: h->profile = value != 0; return SPGEMM_OK;
+        case SPGEMM_OPT_MIN_TRANSPOSE_BIN: h->min_tr_bin = static_cast<int>(value); return SPGEMM_OK;
     }
     return fail(SPGEMM_ERR_INVALID_ARG, "unknown option");
 }
@@ -1112,6 +1329,7 @@ spgemm_status spgemm_get_option(spgemm_handle_t h, spgemm_option opt, int64_t* v
         case SPGEMM_OPT_CLUSTER_SIZE: *value = h->cluster; return SPGEMM_OK;
         case SPGEMM_OPT_STREAMS: *value = h->nside; return SPGEMM_OK;
         case SPGEMM_OPT_PROFILE: *value = h->profile; return SPGEMM_OK;
+        case SPGEMM_OPT_MIN_TRANSPOSE_BIN: *value = h->min_tr_bin; return SPGEMM_OK;
     }
     return fail(SPGEMM_ERR_INVALID_ARG, "unknown option");
 }
@@ -1126,8 +1344,12 @@ spgemm_status spgemm_ladder_info(spgemm_handle_t h, int which, int dtype_bytes, 
         nb = sym1_ladder(&l);
     } else if (which == 1) {
         nb = dtype_bytes == 8 ? s2n_ladder_f64(&l) : s2n_ladder_f32(&l);
-    } else {
+    } else if (which == 2) {
         nb = dtype_bytes == 8 ? s2n_bitmap_ladder_f64(&l) : s2n_bitmap_ladder_f32(&l);
+    } else if (which == 3) {
+        nb = dtype_bytes == 8 ? transpose_ladder_f64(&l) : transpose_ladder_f32(&l);
+    } else {
+        return fail(SPGEMM_ERR_INVALID_ARG, "ladder id must be 0..3");
     }
     *n_bins = nb;
     for (int i = 0; i < 16; i++) limits[i] = i < nb ? l[i].limit : 0;

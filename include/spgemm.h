@@ -167,7 +167,10 @@ typedef enum spgemm_option {
     SPGEMM_OPT_STREAMS = 5,
     /* Record a CUDA event pair around every kernel launch of a product; read
      * the durations with spgemm_last_profile.  0 = off (default), 1 = on. */
-    SPGEMM_OPT_PROFILE = 6
+    SPGEMM_OPT_PROFILE = 6,
+    /* Test knob: every non-empty row of a transpose goes to at least this bin
+     * of its row-sort ladder (-1 = off). */
+    SPGEMM_OPT_MIN_TRANSPOSE_BIN = 7
 } spgemm_option;
 
 SPGEMM_API spgemm_status spgemm_set_option(spgemm_handle_t handle, spgemm_option option, int64_t value);
@@ -191,9 +194,35 @@ SPGEMM_API spgemm_status spgemm_last_profile(spgemm_handle_t handle, spgemm_kern
 /* Number of bins of each ladder and the key limit of bin `bin` (rows whose
  * key -- NIP for the count ladder, nnz for the fill ladders -- is <= limit).
  * which: 0 count ladder; 1 fill ladder used when B.n > 2^20; 2 fill ladder
- * used when B.n <= 2^20 (its large rows use a shared-memory bitmap). */
+ * used when B.n <= 2^20 (its large rows use a shared-memory bitmap);
+ * 3 row-sort ladder of spgemm_transpose_* (key = length of a row of A^T). */
 SPGEMM_API spgemm_status spgemm_ladder_info(spgemm_handle_t handle, int which,
                                  int dtype_bytes, int* n_bins, int64_t* limits /*[16]*/);
+
+/* ---- transpose and the Galerkin triple product ----------------------------- */
+
+/* T = A^T (n x m) as a library-allocated CSR with sorted columns, freed with
+ * spgemm_csr_free.  Values are moved, not computed, so T is exact.  No
+ * counterpart in the reference: its Galerkin use (R = P^T for R*A*P) leaves the
+ * transpose to the caller; here it stays on the device.  Synchronous on
+ * return; one host synchronisation inside. */
+SPGEMM_API spgemm_status spgemm_transpose_f64(spgemm_handle_t handle, const spgemm_csr_view* A,
+                                              spgemm_csr_out* T, void* stream);
+SPGEMM_API spgemm_status spgemm_transpose_f32(spgemm_handle_t handle, const spgemm_csr_view* A,
+                                              spgemm_csr_out* T, void* stream);
+
+/* C = R * (A * P): two chained products (each exactly as spgemm_csr_*), the
+ * intermediate A*P freed before return.  R = NULL means R = P^T, transposed on
+ * the device (then P.m must equal A.m).  Requires A.n == P.m and R.n == A.m.
+ * spgemm_last_info then describes the second product, with `nip` and
+ * `host_syncs` summed over the chain.  Replaces two proposal::proposal calls
+ * (proposal.cuh:85-124) plus a caller-side transpose. */
+SPGEMM_API spgemm_status spgemm_rap_f64(spgemm_handle_t handle, const spgemm_csr_view* R,
+                                        const spgemm_csr_view* A, const spgemm_csr_view* P,
+                                        spgemm_csr_out* C, void* stream);
+SPGEMM_API spgemm_status spgemm_rap_f32(spgemm_handle_t handle, const spgemm_csr_view* R,
+                                        const spgemm_csr_view* A, const spgemm_csr_view* P,
+                                        spgemm_csr_out* C, void* stream);
 
 /* ---- batched products ------------------------------------------------------ */
 

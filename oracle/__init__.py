@@ -117,6 +117,17 @@ def spgemm(A: HostCSR, B: HostCSR, dtype=None) -> HostCSR:
     return HostCSR(A.m, B.n, rpt, col, val)
 
 
+def transpose(A: HostCSR) -> HostCSR:
+    """A^T with sorted columns: a stable counting sort of A's entries by
+    column (entries of one column keep A's row order).  The reference has no
+    transpose; R = P^T of its Galerkin use is formed by the caller."""
+    rows = np.repeat(np.arange(A.m, dtype=np.int32), np.diff(A.rpt))
+    order = np.argsort(A.col, kind="stable")
+    rpt = np.zeros(A.n + 1, dtype=np.int32)
+    np.cumsum(np.bincount(A.col, minlength=A.n), out=rpt[1:])
+    return HostCSR(A.n, A.m, rpt, rows[order].astype(np.int32), A.val[order])
+
+
 def abs_bound(A: HostCSR, B: HostCSR, Cref: HostCSR) -> np.ndarray:
     """Per-entry sum_k |a_ik| |b_kj| over C's structure (FP64)."""
     a_val = np.ascontiguousarray(A.val, dtype=np.float64)

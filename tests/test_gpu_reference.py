@@ -87,3 +87,48 @@ def test_against_reference_build(handle, oracle_mod, name):
     except Exception as e:  # the reference records failed cuSPARSE runs as 0
         rec["cusparse2_error"] = str(e)
     RECORDS[name] = rec
+
+
+def test_galerkin_against_reference_build(handle, oracle_mod):
+    """R * (A * P) on the 27-point stencil of 60^3: the reference runs it as
+    two proposal calls with a host transpose between them; the library as one
+    chained call (R = P^T transposed on the device)."""
+    if not oracle_mod.ref_available():
+        pytest.skip("oracle/_ref not built")
+    import torch
+
+    from gpuspgemm_b200.api import DeviceCSR, rap
+    A = G.stencil27(60)
+    P = G.aggregation_prolongator(60, seed=5)
+    R = oracle_mod.transpose(P)
+    AP_ref = oracle_mod.ref_proposal(A, P, np.float64)
+    C_ref = oracle_mod.ref_proposal(R, AP_ref, np.float64)
+    dA, dP = DeviceCSR.from_host(A), DeviceCSR.from_host(P)
+    for _ in range(3):
+        del_c = rap(dA, dP, None, handle)
+        del del_c
+    ts = []
+    for _ in range(5):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        C = rap(dA, dP, None, handle)
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    C = C.to_host()
+    assert np.array_equal(C.rpt, C_ref.rpt) and np.array_equal(C.col, C_ref.col)
+    # the stencil's rows sum to zero: compare against the magnitude bound
+    absd = lambda M: type(M)(M.m, M.n, M.rpt, M.col, np.abs(M.val))  # noqa: E731
+    bound = oracle_mod.spgemm(absd(R), oracle_mod.spgemm(absd(A), absd(P)))
+    err = float((np.abs(C.val - C_ref.val) / bound.val).max())
+    assert err <= 1e-12, err
+    t_ap, nip_ap = oracle_mod.ref_time("proposal", A, P, np.float64, warmups=3, runs=5)
+    t_rap, nip_rap = oracle_mod.ref_time("proposal", R, AP_ref, np.float64, warmups=3, runs=5)
+    ref_chain = float(np.median(t_ap)) + float(np.median(t_rap))
+    nip = nip_ap + nip_rap
+    RECORDS["galerkin60_f64"] = {
+        "nip": nip, "nnz_C": int(C.nnz), "max_err_vs_reference_over_bound": err,
+        "ours_chain_s": ts, "reference_AP_s": t_ap, "reference_RAP_s": t_rap,
+        "ours_gflops_median": 2 * nip / float(np.median(ts)) / 1e9,
+        "reference_gflops_median_two_calls": 2 * nip / ref_chain / 1e9,
+        "note": "reference time excludes its host transpose of P",
+    }

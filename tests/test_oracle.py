@@ -110,3 +110,21 @@ def test_oracle_against_reference_golden(oracle_mod, name, entry):
         tol = 1e-12 if dt == np.float64 else 1e-5
         # condition-aware bound: |dc| <= tol * sum_k |a_ik||b_kj|
         assert res.get("max_cond", 0.0) <= tol, (which, res)
+
+
+def test_oracle_transpose_matches_scipy():
+    """The oracle's transpose (stable counting sort) against scipy's."""
+    import scipy.sparse as sp
+
+    import oracle
+    from gpuspgemm_b200 import generators as G
+    for A in (G.power_law(3000, 2.0, 300, seed=3), G.uniform_rows(40, 3, seed=3, m=500),
+              G.aggregation_prolongator(9)):
+        T = oracle.transpose(A)
+        S = sp.csr_matrix((A.val, A.col, A.rpt), shape=(A.m, A.n)).T.tocsr()
+        S.sort_indices()
+        assert (T.m, T.n) == S.shape
+        assert np.array_equal(T.rpt, S.indptr) and np.array_equal(T.col, S.indices)
+        assert np.array_equal(T.val, S.data)
+        G2 = G.transpose(A)
+        assert np.array_equal(T.col, G2.col) and np.array_equal(T.val, G2.val)
