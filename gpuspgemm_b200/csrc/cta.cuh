@@ -190,6 +190,25 @@ __device__ __forceinline__ void cta_bitonic_sort(int32_t* s, int N) {
     }
 }
 
+// Move the non-empty slots of table[0, T) to its front, in slot order, by a
+// team of G lanes (T a multiple of G).  Returns the number of keys.  Every
+// lane has read its slot of a chunk before the ballot, and a chunk's writes
+// land below the next chunk's first slot, so the in-place move is safe.
+template<int G>
+__device__ __forceinline__ int team_compact(int32_t* table, int T, unsigned mask, int lane) {
+    const unsigned below = (1u << (threadIdx.x & 31u)) - 1u;
+    int out = 0;
+    for (int base = 0; base < T; base += G) {
+        const int32_t k = table[base + lane];
+        const bool flag = k != kEmpty;
+        const unsigned bits = __ballot_sync(mask, flag) & mask;
+        if (flag) table[out + __popc(bits & below)] = k;
+        out += __popc(bits);
+    }
+    team_sync<G>(mask);
+    return out;
+}
+
 // Ascending bitonic sort of s[0, N) (N a power of two) by a team of G lanes.
 template<int G>
 __device__ __forceinline__ void team_bitonic_sort(int32_t* s, int N, unsigned mask, int lane) {

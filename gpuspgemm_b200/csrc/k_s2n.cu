@@ -29,23 +29,27 @@ __device__ __forceinline__ V ldv(const void* base, int i) {
     return __ldg(static_cast<const V*>(base) + i);
 }
 
-template<typename V, int G, int THREADS, int T, int CAP>
+// Values accumulate straight into the row's slice of C.val with global
+// reductions (fire-and-forget FP64 adds in L2; the row's slice was zeroed by
+// the same team or CTA before the barrier that precedes them).  That keeps no
+// value array in shared memory -- only the key table -- so more rows are in
+// flight per SM, and nothing is copied out at the end.
+
+template<typename V, int G, int THREADS, int T>
 __global__ __launch_bounds__(THREADS) void k_s2n_team(ProductArgs p) {
     constexpr int R = THREADS / G;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    V* s_vals = reinterpret_cast<V*>(smem_raw);
-    int32_t* s_keys = reinterpret_cast<int32_t*>(smem_raw + sizeof(V) * R * CAP);
+    int32_t* s_keys = reinterpret_cast<int32_t*>(smem_raw);
     const int team = threadIdx.x / G;
     const int lane = team_lane<G>();
     const unsigned mask = team_mask<G>();
     const int rid = blockIdx.x * R + team;
     if (rid >= p.nrows) return;
     int32_t* keys = s_keys + team * T;
-    V* vals = s_vals + team * CAP;
     const int row = p.rows[rid];
     const int c0 = p.c_rpt[row];
     const int nnz = p.c_rpt[row + 1] - c0;
-    if (nnz > CAP) {
+    if (nnz > T) {
         if (lane == 0) report(p.status, kStCapacity, row, nnz);
         return;
     }
@@ -57,38 +61,41 @@ __global__ __launch_bounds__(THREADS) void k_s2n_team(ProductArgs p) {
         table_insert(keys, T, __ldg(p.b_col + qb), p.status, row);
     });
     team_sync<G>(mask);
-    team_bitonic_sort<G>(keys, T, mask, lane);
+    // sort only the row's keys: compact them to the front, pad to a power of two
+    const int cnt = team_compact<G>(keys, T, mask, lane);
+    if (cnt != nnz && lane == 0) report(p.status, kStCapacity, row, cnt);
+    const int pn = next_pow2(cnt);
+    for (int i = cnt + lane; i < pn; i += G) keys[i] = kEmpty;
+    team_sync<G>(mask);
+    team_bitonic_sort<G>(keys, pn, mask, lane);
+    V* out = static_cast<V*>(p.c_val) + c0;
     for (int i = lane; i < nnz; i += G) {
         p.c_col[c0 + i] = keys[i];
-        vals[i] = V(0);
+        out[i] = V(0);
     }
     team_sync<G>(mask);
     team_for_products<G>(p.a_col, p.b_rpt, a0, a1, [&](int qb, int ai) {
         const int32_t key = __ldg(p.b_col + qb);
         const int pos = lower_bound_present(keys, nnz, key);
-        atomicAdd(vals + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
+        atomicAdd(out + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
     });
-    team_sync<G>(mask);
-    V* out = static_cast<V*>(p.c_val) + c0;
-    for (int i = lane; i < nnz; i += G) out[i] = vals[i];
 }
 
-template<typename V, int THREADS, int T, int CAP>
+template<int THREADS, int T, int CAP>
 struct CtaLayout {
     static constexpr int P = next_pow2(CAP);
     static constexpr int K = T > P ? T : P;
-    static constexpr size_t vals_bytes = sizeof(V) * CAP;
     static constexpr size_t keys_bytes = sizeof(int32_t) * K;
-    static constexpr size_t bytes = vals_bytes + keys_bytes + sizeof(CtaScratch<THREADS>);
+    static constexpr size_t bytes = keys_bytes + sizeof(CtaScratch<THREADS>);
+    static_assert(bytes <= 232448, "a CTA bin's shared memory exceeds 227 KB");
 };
 
 template<typename V, int THREADS, int T, int CAP>
 __global__ __launch_bounds__(THREADS) void k_s2n_cta(ProductArgs p) {
-    using L = CtaLayout<V, THREADS, T, CAP>;
+    using L = CtaLayout<THREADS, T, CAP>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    V* vals = reinterpret_cast<V*>(smem_raw);
-    int32_t* keys = reinterpret_cast<int32_t*>(smem_raw + L::vals_bytes);
-    auto& sc = *reinterpret_cast<CtaScratch<THREADS>*>(smem_raw + L::vals_bytes + L::keys_bytes);
+    int32_t* keys = reinterpret_cast<int32_t*>(smem_raw);
+    auto& sc = *reinterpret_cast<CtaScratch<THREADS>*>(smem_raw + L::keys_bytes);
     const int row = p.rows[blockIdx.x];
     const int c0 = p.c_rpt[row];
     const int nnz = p.c_rpt[row + 1] - c0;
@@ -109,18 +116,17 @@ __global__ __launch_bounds__(THREADS) void k_s2n_cta(ProductArgs p) {
     for (int i = nnz + threadIdx.x; i < pn; i += THREADS) keys[i] = kEmpty;
     __syncthreads();
     cta_bitonic_sort<THREADS>(keys, pn);
+    V* out = static_cast<V*>(p.c_val) + c0;
     for (int i = threadIdx.x; i < nnz; i += THREADS) {
         p.c_col[c0 + i] = keys[i];
-        vals[i] = V(0);
+        out[i] = V(0);
     }
     __syncthreads();
     cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int ai) {
         const int32_t key = __ldg(p.b_col + qb);
         const int pos = lower_bound_present(keys, nnz, key);
-        atomicAdd(vals + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
+        atomicAdd(out + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
     });
-    V* out = static_cast<V*>(p.c_val) + c0;
-    for (int i = threadIdx.x; i < nnz; i += THREADS) out[i] = vals[i];
 }
 
 // Bitmap bin (B.n <= kBitmapCols): the row's hash table is the identity hash
@@ -294,24 +300,23 @@ __global__ __launch_bounds__(THREADS) void k_s2n_global(ProductArgs p) {
     }
 }
 
-template<typename V, int G, int THREADS, int T, int CAP>
+template<int G, int THREADS, int T>
 constexpr size_t team_smem() {
-    return (sizeof(V) * CAP + sizeof(int32_t) * T) * (THREADS / G);
+    return sizeof(int32_t) * T * (THREADS / G);
 }
 
-template<typename V, int G, int THREADS, int T, int CAP>
+template<typename V, int G, int THREADS, int T>
 cudaError_t launch_team(const ProductArgs& p, cudaStream_t s) {
     constexpr int R = THREADS / G;
     const int grid = (p.nrows + R - 1) / R;
-    k_s2n_team<V, G, THREADS, T, CAP>
-        <<<grid, THREADS, team_smem<V, G, THREADS, T, CAP>(), s>>>(p);
+    k_s2n_team<V, G, THREADS, T><<<grid, THREADS, team_smem<G, THREADS, T>(), s>>>(p);
     return cudaGetLastError();
 }
 
 template<typename V, int THREADS, int T, int CAP>
 cudaError_t launch_cta(const ProductArgs& p, cudaStream_t s) {
     k_s2n_cta<V, THREADS, T, CAP>
-        <<<p.nrows, THREADS, CtaLayout<V, THREADS, T, CAP>::bytes, s>>>(p);
+        <<<p.nrows, THREADS, CtaLayout<THREADS, T, CAP>::bytes, s>>>(p);
     return cudaGetLastError();
 }
 
@@ -338,20 +343,20 @@ struct S2nLadder {
 #define B200_S2N_LADDER(V)                                                                    \
     template<>                                                                                \
     const BinLauncher S2nLadder<V>::entries[] = {                                             \
-        {BinKind::Team, 12, 64, 256, team_smem<V, 4, 256, 16, 12>(), "s2n_team4_t16",         \
-         launch_team<V, 4, 256, 16, 12>},                                                     \
-        {BinKind::Team, 48, 32, 256, team_smem<V, 8, 256, 64, 48>(), "s2n_team8_t64",         \
-         launch_team<V, 8, 256, 64, 48>},                                                     \
-        {BinKind::Team, 192, 16, 256, team_smem<V, 16, 256, 256, 192>(), "s2n_team16_t256",   \
-         launch_team<V, 16, 256, 256, 192>},                                                  \
-        {BinKind::Team, 768, 8, 256, team_smem<V, 32, 256, 1024, 768>(), "s2n_team32_t1024",  \
-         launch_team<V, 32, 256, 1024, 768>},                                                 \
-        {BinKind::Cta, 3072, 1, 256, CtaLayout<V, 256, 4096, 3072>::bytes, "s2n_cta256_t4096", \
+        {BinKind::Team, 12, 64, 256, team_smem<4, 256, 16>(), "s2n_team4_t16",                \
+         launch_team<V, 4, 256, 16>},                                                         \
+        {BinKind::Team, 48, 32, 256, team_smem<8, 256, 64>(), "s2n_team8_t64",                \
+         launch_team<V, 8, 256, 64>},                                                         \
+        {BinKind::Team, 192, 16, 256, team_smem<16, 256, 256>(), "s2n_team16_t256",           \
+         launch_team<V, 16, 256, 256>},                                                       \
+        {BinKind::Team, 768, 8, 256, team_smem<32, 256, 1024>(), "s2n_team32_t1024",          \
+         launch_team<V, 32, 256, 1024>},                                                      \
+        {BinKind::Cta, 3072, 1, 256, CtaLayout<256, 4096, 3072>::bytes, "s2n_cta256_t4096",   \
          launch_cta<V, 256, 4096, 3072>},                                                     \
-        {BinKind::Cta, 12288, 1, 512, CtaLayout<V, 512, 16384, 12288>::bytes,                 \
+        {BinKind::Cta, 12288, 1, 512, CtaLayout<512, 16384, 12288>::bytes,                    \
          "s2n_cta512_t16384", launch_cta<V, 512, 16384, 12288>},                              \
-        {BinKind::Cta, 16384, 1, 1024, CtaLayout<V, 1024, 20480, 16384>::bytes,               \
-         "s2n_cta1024_t20480", launch_cta<V, 1024, 20480, 16384>},                            \
+        {BinKind::Cta, 32768, 1, 1024, CtaLayout<1024, 43008, 32768>::bytes,                  \
+         "s2n_cta1024_t43008", launch_cta<V, 1024, 43008, 32768>},                            \
         {BinKind::Global, INT32_MAX, 1, 1024, 0, "s2n_global_bitmap", launch_global<V, 1024>}, \
     };                                                                                        \
     template<>                                                                                \
@@ -393,13 +398,13 @@ cudaError_t prepare_one() {
     if (e == cudaSuccess)                                                                 \
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
                                  static_cast<int>(bytes));
-    B200_SMEM((k_s2n_team<V, 4, 256, 16, 12>), (team_smem<V, 4, 256, 16, 12>()));
-    B200_SMEM((k_s2n_team<V, 8, 256, 64, 48>), (team_smem<V, 8, 256, 64, 48>()));
-    B200_SMEM((k_s2n_team<V, 16, 256, 256, 192>), (team_smem<V, 16, 256, 256, 192>()));
-    B200_SMEM((k_s2n_team<V, 32, 256, 1024, 768>), (team_smem<V, 32, 256, 1024, 768>()));
-    B200_SMEM((k_s2n_cta<V, 256, 4096, 3072>), (CtaLayout<V, 256, 4096, 3072>::bytes));
-    B200_SMEM((k_s2n_cta<V, 512, 16384, 12288>), (CtaLayout<V, 512, 16384, 12288>::bytes));
-    B200_SMEM((k_s2n_cta<V, 1024, 20480, 16384>), (CtaLayout<V, 1024, 20480, 16384>::bytes));
+    B200_SMEM((k_s2n_team<V, 4, 256, 16>), (team_smem<4, 256, 16>()));
+    B200_SMEM((k_s2n_team<V, 8, 256, 64>), (team_smem<8, 256, 64>()));
+    B200_SMEM((k_s2n_team<V, 16, 256, 256>), (team_smem<16, 256, 256>()));
+    B200_SMEM((k_s2n_team<V, 32, 256, 1024>), (team_smem<32, 256, 1024>()));
+    B200_SMEM((k_s2n_cta<V, 256, 4096, 3072>), (CtaLayout<256, 4096, 3072>::bytes));
+    B200_SMEM((k_s2n_cta<V, 512, 16384, 12288>), (CtaLayout<512, 16384, 12288>::bytes));
+    B200_SMEM((k_s2n_cta<V, 1024, 43008, 32768>), (CtaLayout<1024, 43008, 32768>::bytes));
     B200_SMEM((k_s2n_bitmap<V, 1024, 16384>), (BitmapLayout<V, 1024, 16384>::bytes));
 #undef B200_SMEM
     return e;
