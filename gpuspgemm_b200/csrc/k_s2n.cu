@@ -17,6 +17,7 @@
 
 #include "cta.cuh"
 #include "kernels.hpp"
+#include "sort.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -61,22 +62,20 @@ __global__ __launch_bounds__(THREADS) void k_s2n_team(ProductArgs p) {
         table_insert(keys, T, __ldg(p.b_col + qb), p.status, row);
     });
     team_sync<G>(mask);
-    // sort only the row's keys: compact them to the front, pad to a power of two
+    // sort only the row's keys: compact them to the front, then the register
+    // sort leaves them in swizzled order (sort.cuh)
     const int cnt = team_compact<G>(keys, T, mask, lane);
     if (cnt != nnz && lane == 0) report(p.status, kStCapacity, row, cnt);
-    const int pn = next_pow2(cnt);
-    for (int i = cnt + lane; i < pn; i += G) keys[i] = kEmpty;
-    team_sync<G>(mask);
-    team_bitonic_sort<G>(keys, pn, mask, lane);
+    team_sort_swz<G, T / G>(keys, cnt, mask, lane);
     V* out = static_cast<V*>(p.c_val) + c0;
     for (int i = lane; i < nnz; i += G) {
-        p.c_col[c0 + i] = keys[i];
+        p.c_col[c0 + i] = keys[swz(i)];
         out[i] = V(0);
     }
     team_sync<G>(mask);
     team_for_products<G>(p.a_col, p.b_rpt, a0, a1, [&](int qb, int ai) {
         const int32_t key = __ldg(p.b_col + qb);
-        const int pos = lower_bound_present(keys, nnz, key);
+        const int pos = lower_bound_present_swz(keys, nnz, key);
         atomicAdd(out + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
     });
 }
