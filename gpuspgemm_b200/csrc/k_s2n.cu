@@ -111,19 +111,20 @@ __global__ __launch_bounds__(THREADS) void k_s2n_cta(ProductArgs p) {
     });
     const int cnt = cta_compact<THREADS>(keys, T, sc.warp_tot);
     if (cnt != nnz && threadIdx.x == 0) report(p.status, kStCapacity, row, cnt);
-    const int pn = next_pow2(nnz);
-    for (int i = nnz + threadIdx.x; i < pn; i += THREADS) keys[i] = kEmpty;
-    __syncthreads();
-    cta_bitonic_sort<THREADS>(keys, pn);
+    // register sort of the row's keys; they come back in swizzled order
+    static_assert(L::K >= THREADS * 16, "the register sort needs THREADS * 16 key slots");
+    // (cnt > CAP only for an invalid operand, reported above; the clamp keeps
+    // the sort inside the K key slots)
+    cta_sort_swz<THREADS>(keys, cnt <= CAP ? cnt : CAP);
     V* out = static_cast<V*>(p.c_val) + c0;
     for (int i = threadIdx.x; i < nnz; i += THREADS) {
-        p.c_col[c0 + i] = keys[i];
+        p.c_col[c0 + i] = keys[swz(i)];
         out[i] = V(0);
     }
     __syncthreads();
     cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int ai) {
         const int32_t key = __ldg(p.b_col + qb);
-        const int pos = lower_bound_present(keys, nnz, key);
+        const int pos = lower_bound_present_swz(keys, nnz, key);
         atomicAdd(out + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
     });
 }

@@ -15,7 +15,7 @@
 // search) all bank-conflict free within a 32-lane team.
 #pragma once
 
-#include "common.cuh"
+#include "cta.cuh"
 
 namespace b200 {
 
@@ -95,6 +95,113 @@ __device__ __forceinline__ void team_sort_swz(int32_t* keys, int n, unsigned mas
         if constexpr (EMAX >= 16) team_sort_regs<G, 16>(keys, n, mask, lane);
     } else {
         if constexpr (EMAX >= 32) team_sort_regs<G, 32>(keys, n, mask, lane);
+    }
+}
+
+// In-lane steps j < E of stage k: elements e and e + j; ascending iff bit k of
+// the element's index (lane * E + e) is clear.
+template<int E>
+__device__ __forceinline__ void lane_steps(int32_t (&r)[E], int k, int base) {
+#pragma unroll
+    for (int j = E / 2; j > 0; j >>= 1) {
+        if (j < k) {
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                if ((e & j) == 0) {
+                    const bool up = ((base + e) & k) == 0;
+                    const int32_t a = r[e];
+                    const int32_t b = r[e + j];
+                    r[e] = up ? min(a, b) : max(a, b);
+                    r[e + j] = up ? max(a, b) : min(a, b);
+                }
+            }
+        }
+    }
+}
+
+// The same network over a whole CTA: THREADS threads with E keys each.
+// Steps closer than E stay in registers, steps up to 32 * E pair lanes of one
+// warp through shuffles, and only the wider steps (log2(THREADS / 32) levels,
+// a handful of stages) exchange through shared memory, in swizzled order.
+// Unlike the team network, the stage loops run at run time: the CTA kernels
+// run beside the team kernels, and fully unrolled copies of this network for
+// every E measured slower on the 1M power-law product (code size and
+// registers).  keys[] must hold at least THREADS * E slots.  All threads must
+// call it.
+template<int THREADS, int E>
+__device__ __forceinline__ void cta_sort_regs(int32_t* keys, int n) {
+    constexpr int N = THREADS * E;
+    const int tid = threadIdx.x;
+    int32_t r[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+        const int i = e * THREADS + tid;
+        r[e] = i < n ? keys[i] : kEmpty;
+    }
+    __syncthreads();  // every thread has read its input keys
+#pragma unroll 1
+    for (int k = 2; k <= N; k <<= 1) {
+        const bool up = ((tid * E) & k) == 0;
+#pragma unroll 1
+        for (int j = k >> 1; j >= E; j >>= 1) {
+            const int d = j / E;
+            const bool keep_min = ((tid & d) == 0) == up;
+            if (d < 32) {
+#pragma unroll
+                for (int e = 0; e < E; e++) {
+                    const int32_t o = __shfl_xor_sync(0xffffffffu, r[e], d);
+                    r[e] = keep_min ? min(r[e], o) : max(r[e], o);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < E; e++) keys[swz(tid * E + e)] = r[e];
+                __syncthreads();
+#pragma unroll
+                for (int e = 0; e < E; e++) {
+                    const int32_t o = keys[swz((tid ^ d) * E + e)];
+                    r[e] = keep_min ? min(r[e], o) : max(r[e], o);
+                }
+                __syncthreads();
+            }
+        }
+        lane_steps<E>(r, k, tid * E);
+    }
+#pragma unroll
+    for (int e = 0; e < E; e++) keys[swz(tid * E + e)] = r[e];
+    __syncthreads();
+}
+
+// Sort keys[0, n) of a CTA into swizzled order.  Rows of up to THREADS * 16
+// keys use the register network; longer ones (the largest CTA bins) run the
+// shared-memory bitonic network on keys[0, next_pow2(n)) and are then
+// swizzled in place -- swz only permutes inside 32-key blocks and is its own
+// inverse, so each warp swaps within its blocks with no CTA barrier between
+// its read and its write.  keys[] must hold next_pow2(n) and THREADS * 16 slots.
+template<int THREADS>
+__device__ __forceinline__ void cta_sort_swz(int32_t* keys, int n) {
+    const int e = (n + THREADS - 1) / THREADS;
+    if (e <= 1) {
+        cta_sort_regs<THREADS, 1>(keys, n);
+    } else if (e <= 2) {
+        cta_sort_regs<THREADS, 2>(keys, n);
+    } else if (e <= 4) {
+        cta_sort_regs<THREADS, 4>(keys, n);
+    } else if (e <= 8) {
+        cta_sort_regs<THREADS, 8>(keys, n);
+    } else if (e <= 16) {
+        cta_sort_regs<THREADS, 16>(keys, n);
+    } else {
+        const int pn = next_pow2(n);
+        for (int i = n + threadIdx.x; i < pn; i += THREADS) keys[i] = kEmpty;
+        __syncthreads();
+        cta_bitonic_sort<THREADS>(keys, pn);
+        const int lane = threadIdx.x & 31;
+        for (int b = (threadIdx.x >> 5) * 32; b < pn; b += THREADS) {
+            const int32_t v = keys[b + lane];
+            __syncwarp();
+            keys[swz(b + lane)] = v;
+        }
+        __syncthreads();
     }
 }
 

@@ -172,6 +172,26 @@ def _block_diag(mats):
                    np.concatenate(cols).astype(np.int32), np.concatenate(vals))
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_long_rows_wide_cta_bins(handle, oracle_mod, dtype):
+    """Rows of ~20.7k, ~12k and ~2.4k distinct columns of a B with 2^21 + 7
+    columns: the hash CTA bins' register sort (up to 16 keys per thread) and
+    its shared-memory fallback for longer rows."""
+    rng = np.random.default_rng(11)
+    nb, n = 2600, (1 << 21) + 7
+    b_rows = [np.unique(rng.integers(0, n, 8)) for _ in range(nb)]
+    B = HostCSR(nb, n, np.concatenate([[0], np.cumsum([len(r) for r in b_rows])]).astype(np.int32),
+                np.concatenate(b_rows).astype(np.int32),
+                rng.uniform(0.1, 1, sum(len(r) for r in b_rows)))
+    cols = [np.arange(nb), np.sort(rng.choice(nb, 1500, replace=False)),
+            np.sort(rng.choice(nb, 300, replace=False))]
+    A = HostCSR(3, nb, np.concatenate([[0], np.cumsum([len(c) for c in cols])]).astype(np.int32),
+                np.concatenate(cols).astype(np.int32), rng.uniform(0.1, 1, sum(map(len, cols))))
+    C = gpu_product(A, B, handle, dtype)
+    assert int(np.diff(C.rpt).max()) > 16384
+    check(oracle_mod, A, B, C, dtype, "long_rows_wide", positive=True)
+
+
 def test_heavy_row_spills_to_global(handle, oracle_mod):
     """One row with ~190k distinct columns: past the cluster table, so the
     count spills to the global bitmap and the fill runs in the global bin."""
