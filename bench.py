@@ -37,6 +37,14 @@ sys.path.insert(0, str(ROOT))
 METRIC = "C=A*A GFLOPS (2*NIP/s), power-law n=1e6 FP64"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic
+# byte of a fill kernel, from one ncu capture of the power-law n = 200,000
+# case (profiles/s2n_fused_powerlaw200k_f64.md: 10.84 MB read + 0.008 MB
+# written against 20.80 MB algorithmic for the same launch).  The capture is
+# scaled to the launch the bench reports by its algorithmic bytes: at both
+# sizes A and B fit in L2, so DRAM reads are the first touch of A's and B's
+# rows and C's writes drain from L2 after the kernel.
+TRAFFIC_PER_ALG_BYTE = {"s2n_team32_t1024": (10844160 + 7680) / 20804236}
 
 
 def parse():
@@ -348,7 +356,11 @@ def run_ours(args, rank, world, local_rank):
         "bound": "hbm", "kernel": name, "phase": int(phase), "bin": int(b),
         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
         "peak_source": "MEASURED_PEAKS.json" if PEAKS_FILE.exists() else "fallback",
-        "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg[dom], "traffic": None,
+        "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg[dom],
+        "traffic": (TRAFFIC_PER_ALG_BYTE[name] * alg_bytes if name in TRAFFIC_PER_ALG_BYTE
+                    else None),
+        "traffic_source": ("ncu dram bytes of the n=200k case, scaled by algorithmic bytes"
+                           if name in TRAFFIC_PER_ALG_BYTE else None),
         "whole_product": {"alg_bytes": whole_bytes,
                           "achieved_gbs": whole_bytes / (step_ms_avg / 1e3) / 1e9},
     }

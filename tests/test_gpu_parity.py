@@ -192,6 +192,16 @@ def test_long_rows_wide_cta_bins(handle, oracle_mod, dtype):
     check(oracle_mod, A, B, C, dtype, "long_rows_wide", positive=True)
 
 
+def test_high_compression_stencil(handle, oracle_mod):
+    """A 27-point stencil squared: ~5.9 products per entry of C, all
+    accumulated with global reductions into the row's slice of C.val."""
+    S = G.stencil27(20)
+    C = gpu_product(S, S, handle, np.float64)
+    info = handle.info()
+    assert info["nip"] > 5 * info["nnz"]
+    check(oracle_mod, S, S, C, np.float64, "stencil20_squared")
+
+
 def test_heavy_row_spills_to_global(handle, oracle_mod):
     """One row with ~190k distinct columns: past the cluster table, so the
     count spills to the global bitmap and the fill runs in the global bin."""
