@@ -651,6 +651,8 @@ def run_served(args, local_rank):
             r.done.wait()
         span = max(r.t_done for r in reqs) - t_start
         bad = [r for r in reqs if r.error is not None]
+        for r in reqs:  # keep the timings, free the results before the next run
+            r.result = None
         tl = server.timeline
         batches = {"units": len(tl), "batched": sum(1 for u in tl if u[1] > 1),
                    "alone": sum(1 for u in tl if u[1] == 1),

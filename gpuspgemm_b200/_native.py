@@ -114,6 +114,8 @@ SIGNATURES = {
     "spgemm_host_csr_free": (C.c_int, [C.POINTER(CsrOut)]),
     "spgemm_get_nip": (C.c_int, [C.c_void_p, C.POINTER(CsrView), C.POINTER(CsrView),
                                  C.POINTER(C.c_int64), C.c_void_p]),
+    "spgemm_get_nip_many": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(CsrView),
+                                      C.POINTER(CsrView), C.POINTER(C.c_int64), C.c_void_p]),
     "spgemm_last_info": (C.c_int, [C.c_void_p, C.POINTER(Info)]),
     "spgemm_last_profile": (C.c_int, [C.c_void_p, C.POINTER(KernelTime), C.c_int32,
                                       C.POINTER(C.c_int32)]),

@@ -393,6 +393,21 @@ def proposal_host(A: HostCSR, B: HostCSR, handle: Handle | None = None,
     return HostCSR(m, n, rpt, col, val)
 
 
+def get_nip_many(pairs, handle: Handle | None = None, stream=None) -> list[int]:
+    """NIP of many (A_i, B_i) pairs with one launch and one host sync
+    (spgemm_get_nip_many); the reference sizes one pair per call
+    (utils::get_nip, nip.cuh:52-78)."""
+    h = handle or default_handle()
+    n = len(pairs)
+    if n == 0:
+        return []
+    va = (N.CsrView * n)(*[a.view() for a, _ in pairs])
+    vb = (N.CsrView * n)(*[b.view() for _, b in pairs])
+    out = (C.c_int64 * n)()
+    N.check(N.lib().spgemm_get_nip_many(h.ptr, n, va, vb, out, _stream_ptr(stream)))
+    return [int(x) for x in out]
+
+
 def transpose(A: DeviceCSR, handle: Handle | None = None, stream=None) -> DeviceCSR:
     """A^T on the device, columns sorted (spgemm_transpose_*).  The reference
     has no transpose; its Galerkin use forms R = P^T outside the library."""

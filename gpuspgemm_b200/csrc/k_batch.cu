@@ -60,7 +60,56 @@ __global__ __launch_bounds__(kBatchThreads) void k_unpack(
     for (int p = p0 + threadIdx.x; p < p1; p += kBatchThreads) c_col[p] -= shift;
 }
 
+// NIP of many independent pairs (A_i, B_i) in one launch: pair i's A entries
+// are cut into chunks of kNipChunk, one CTA per chunk (cta_off[i] is pair i's
+// first CTA); each CTA sums len(B_i(k,:)) over its entries and adds the total
+// to nip[i] (zeroed by the caller) with one atomic.
+constexpr int kNipChunk = 16384;
+
+__global__ __launch_bounds__(kBatchThreads) void k_pairs_nip(const NipPair* __restrict__ pairs,
+                                                            const int32_t* __restrict__ cta_off,
+                                                            int32_t count,
+                                                            long long* __restrict__ nip) {
+    __shared__ long long s_part[kBatchThreads / kWarp];
+    const int b = blockIdx.x;
+    // the pair this CTA belongs to: the last i with cta_off[i] <= b
+    int lo = 0;
+    int hi = count;  // cta_off[count] > b
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (cta_off[mid] <= b) lo = mid;
+        else hi = mid;
+    }
+    const NipPair pr = pairs[lo];
+    const int e0 = (b - cta_off[lo]) * kNipChunk;
+    const int e1 = min(e0 + kNipChunk, pr.nnz);
+    long long s = 0;
+    for (int e = e0 + threadIdx.x; e < e1; e += kBatchThreads) {
+        const int c = __ldg(pr.a_col + e);
+        s += __ldg(pr.b_rpt + c + 1) - __ldg(pr.b_rpt + c);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long t = 0;
+        for (int w = 0; w < kBatchThreads / kWarp; w++) t += s_part[w];
+        atomicAdd(reinterpret_cast<unsigned long long*>(nip + lo),
+                  static_cast<unsigned long long>(t));
+    }
+}
+
 }  // namespace
+
+int32_t pairs_nip_ctas(int32_t nnz) { return (nnz + kNipChunk - 1) / kNipChunk; }
+
+cudaError_t launch_pairs_nip(const NipPair* pairs, const int32_t* cta_off, int32_t count,
+                             int32_t ctas, long long* nip, cudaStream_t s) {
+    if (ctas <= 0) return cudaSuccess;
+    k_pairs_nip<<<ctas, kBatchThreads, 0, s>>>(pairs, cta_off, count, nip);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_product_nip(const int32_t* a_rpt, const int32_t* a_col, const int32_t* b_rpt,
                                const int32_t* row_off, int32_t count, long long* nip,

@@ -127,6 +127,16 @@ cudaError_t launch_col_count(const int32_t* col, int32_t nnz, int32_t n, int32_t
 cudaError_t launch_tr_scatter(const int32_t* a_rpt, const int32_t* a_col, int32_t m, int32_t n,
                               const int32_t* t_rpt, int32_t* cursor, uint64_t* keys,
                               cudaStream_t s);
+// NIP of many independent pairs in one launch (spgemm_get_nip_many).
+struct NipPair {
+    const int32_t* a_col;   // A_i's column indices (nnz entries)
+    const int32_t* b_rpt;   // B_i's row pointer
+    int32_t nnz;            // nnz(A_i)
+    int32_t pad;
+};
+int32_t pairs_nip_ctas(int32_t nnz);  // CTAs the launch gives one pair
+cudaError_t launch_pairs_nip(const NipPair* pairs, const int32_t* cta_off, int32_t count,
+                             int32_t ctas, long long* nip, cudaStream_t s);
 // Total NIP only (spgemm_get_nip).
 cudaError_t launch_total_nip(const int32_t* a_rpt, const int32_t* a_col, const int32_t* b_rpt,
                              int32_t m, long long* out, cudaStream_t s);

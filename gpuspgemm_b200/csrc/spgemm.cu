@@ -1066,9 +1066,18 @@ spgemm_status rap(spgemm_handle_s* h, const spgemm_csr_view* R, const spgemm_csr
 // created on first use and never destroyed: results may outlive the handle
 // that made them, and a pool must not go away under live allocations.  Its
 // release threshold is the maximum, so freed memory stays mapped for the next
-// product (trimmed when a handle is destroyed).
+// product.  It is trimmed only when the last handle on its device goes away:
+// trimming under other live handles would make their next products re-map
+// their memory.
 std::mutex g_pool_mu;
 cudaMemPool_t g_pools[64] = {};
+int g_pool_users[64] = {};
+
+void release_pool(int dev) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (dev < 0 || dev >= 64 || g_pools[dev] == nullptr) return;
+    if (--g_pool_users[dev] == 0) cudaMemPoolTrimTo(g_pools[dev], 0);
+}
 
 spgemm_status device_pool(int dev, cudaMemPool_t* out) {
     if (dev < 0 || dev >= 64) return fail(SPGEMM_ERR_INVALID_ARG, "device ordinal out of range");
@@ -1084,6 +1093,7 @@ spgemm_status device_pool(int dev, cudaMemPool_t* out) {
         B200_TRY(cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep));
         g_pools[dev] = p;
     }
+    g_pool_users[dev]++;
     *out = g_pools[dev];
     return SPGEMM_OK;
 }
@@ -1162,8 +1172,8 @@ spgemm_status spgemm_destroy(spgemm_handle_t h) {
     if (h->mirror) cudaFreeHost(h->mirror);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     // the pool is shared and outlives handles (results may outlive them too);
-    // give its unused cached memory back
-    if (h->pool) cudaMemPoolTrimTo(h->pool, 0);
+    // the last handle on the device gives its unused cached memory back
+    if (h->pool) release_pool(h->device);
     delete h;
     return SPGEMM_OK;
 }
@@ -1279,6 +1289,56 @@ spgemm_status spgemm_get_nip(spgemm_handle_t h, const spgemm_csr_view* A,
     B200_TRY(cudaStreamSynchronize(s));
     v = h->mirror->plan.total_key;
     *nip = v;
+    return SPGEMM_OK;
+}
+
+spgemm_status spgemm_get_nip_many(spgemm_handle_t h, int32_t count, const spgemm_csr_view* A,
+                                  const spgemm_csr_view* B, int64_t* nip, void* stream) {
+    if (h == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "handle is NULL");
+    if (count < 0) return fail(SPGEMM_ERR_INVALID_ARG, "negative count");
+    if (count == 0) return SPGEMM_OK;
+    if (A == nullptr || B == nullptr || nip == nullptr)
+        return fail(SPGEMM_ERR_INVALID_ARG, "NULL argument");
+    std::vector<NipPair> pairs(count);
+    std::vector<int32_t> cta_off(size_t(count) + 1);
+    int64_t ctas = 0;
+    for (int32_t i = 0; i < count; i++) {
+        if (spgemm_status st = check_view(A + i, "A[i]"); st != SPGEMM_OK) return st;
+        if (spgemm_status st = check_view(B + i, "B[i]"); st != SPGEMM_OK) return st;
+        if (A[i].n != B[i].m)
+            return fail(SPGEMM_ERR_INVALID_ARG,
+                        "A[" + std::to_string(i) + "].n must equal B[" + std::to_string(i) + "].m");
+        pairs[i] = NipPair{A[i].col, B[i].rpt, A[i].nnz, 0};
+        cta_off[i] = static_cast<int32_t>(ctas);
+        ctas += pairs_nip_ctas(A[i].nnz);
+        if (ctas > INT32_MAX) return fail(SPGEMM_ERR_OVERFLOW, "too many entries in one call");
+    }
+    cta_off[count] = static_cast<int32_t>(ctas);
+    B200_TRY(cudaSetDevice(h->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t o_pairs = 0;
+    const size_t o_off = align_up(o_pairs + sizeof(NipPair) * size_t(count), 256);
+    const size_t o_nip = align_up(o_off + sizeof(int32_t) * (size_t(count) + 1), 256);
+    const size_t bytes = o_nip + sizeof(long long) * size_t(count);
+    char* d = nullptr;
+    B200_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&d), bytes, h->pool, s));
+    cudaError_t e = cudaMemcpyAsync(d + o_pairs, pairs.data(), sizeof(NipPair) * size_t(count),
+                                    cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d + o_off, cta_off.data(), sizeof(int32_t) * (size_t(count) + 1),
+                            cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d + o_nip, 0, sizeof(long long) * size_t(count), s);
+    if (e == cudaSuccess)
+        e = launch_pairs_nip(reinterpret_cast<const NipPair*>(d + o_pairs),
+                             reinterpret_cast<const int32_t*>(d + o_off), count,
+                             static_cast<int32_t>(ctas), reinterpret_cast<long long*>(d + o_nip), s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(nip, d + o_nip, sizeof(long long) * size_t(count),
+                            cudaMemcpyDeviceToHost, s);
+    const cudaError_t ef = cudaFreeAsync(d, s);
+    if (e == cudaSuccess) e = ef;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "get_nip_many");
     return SPGEMM_OK;
 }
 

@@ -4,8 +4,8 @@ Requests ``C = A * B`` (operands already on the device) arrive at any time.
 Worker threads, each owning a library handle (its own side streams, scratch and
 stream), repeatedly
 
-1. size new arrivals on the device: NIP (intermediate products) of each, in
-   small chunks so that admission starts before a burst is fully sized; the
+1. size new arrivals on the device: NIP (intermediate products) of all of
+   them with one launch and one host synchronisation (spgemm_get_nip_many); the
    binning phase's upper bound on the output,
    ``bytes(C) <= 4 (m + 1) + NIP * (4 + sizeof(value))``, is the request's
    share of the memory budget;
@@ -33,7 +33,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .api import DeviceCSR, Handle, PackedBatch, batch, get_nip, pack_batch, proposal
+from .api import DeviceCSR, Handle, PackedBatch, batch, get_nip_many, pack_batch, proposal
 
 
 @dataclass
@@ -66,12 +66,13 @@ class SpgemmServer:
                    alone on the plain path.
     batch_nip:     cap on the intermediate products of one batch (bounds the
                    time a batch's first request waits for its last).
-    size_chunk:    arrivals a worker sizes before it tries to admit.
+    size_chunk:    most arrivals a worker sizes in one call before it tries to
+                   admit.
     """
 
     def __init__(self, memory_budget: int = 32 << 30, max_batch: int = 256, workers: int = 2,
                  device: int = 0, solo_nip: int = 4 << 20, batch_nip: int = 32 << 20,
-                 size_chunk: int = 16):
+                 size_chunk: int = 256):
         import torch
         self._torch = torch
         self.device = device
@@ -175,14 +176,17 @@ class SpgemmServer:
                         if len(unsized) == self.size_chunk:
                             break
             if unsized:
-                # admission bounds of new arrivals, on this worker's stream
-                for r in unsized:
-                    try:
-                        r.nip = get_nip(r.A, r.B, handle, stream)
-                    except BaseException as e:
+                # admission bounds of new arrivals: one sizing launch, on this
+                # worker's stream
+                try:
+                    nips = get_nip_many([(r.A, r.B) for r in unsized], handle, stream)
+                except BaseException as e:  # an invalid pair fails the whole call
+                    nips = [0] * len(unsized)
+                    for r in unsized:
                         r.error = e
-                        r.nip = 0
-                    r.bound_bytes = 4 * (r.A.m + 1) + r.nip * (4 + r.A.val.element_size())
+                for r, nip in zip(unsized, nips):
+                    r.nip = nip
+                    r.bound_bytes = 4 * (r.A.m + 1) + nip * (4 + r.A.val.element_size())
                 with self._cv:
                     self._cv.notify_all()
             with self._cv:

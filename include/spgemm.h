@@ -146,6 +146,16 @@ SPGEMM_API spgemm_status spgemm_host_csr_free(spgemm_csr_out* C);
 SPGEMM_API spgemm_status spgemm_get_nip(spgemm_handle_t handle, const spgemm_csr_view* A,
                              const spgemm_csr_view* B, int64_t* nip, void* stream);
 
+/* NIP of `count` independent pairs (A[i], B[i]) in one launch and one host
+ * synchronisation: nip[i] = sum over A[i]'s entries (r, k) of nnz(B[i](k,:)).
+ * A, B and nip are HOST arrays of count entries; the views' arrays are on the
+ * device.  For callers that size many products at once (the served form's
+ * admission); the reference sizes one pair per call (utils::get_nip,
+ * nip.cuh:52-78). */
+SPGEMM_API spgemm_status spgemm_get_nip_many(spgemm_handle_t handle, int32_t count,
+                                             const spgemm_csr_view* A, const spgemm_csr_view* B,
+                                             int64_t* nip, void* stream);
+
 /* Statistics of the last product run on `handle`. */
 SPGEMM_API spgemm_status spgemm_last_info(spgemm_handle_t handle, spgemm_info* info);
 

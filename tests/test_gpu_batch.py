@@ -69,3 +69,25 @@ def test_batch_packed_gpu_generator_and_groups(handle, oracle_mod):
         assert res["max_cond"] <= 1e-5, res
     assert handle._last_groups >= 1
     torch.cuda.synchronize()
+
+
+def test_get_nip_many_matches_single_calls(handle, oracle_mod):
+    """One-launch sizing of many pairs: empty A, a pair larger than one CTA's
+    chunk (16384 A entries), rectangular pairs."""
+    import numpy as np
+
+    from gpuspgemm_b200 import generators as G
+    from gpuspgemm_b200.api import DeviceCSR, get_nip, get_nip_many
+    from gpuspgemm_b200.csr import HostCSR
+    mats = [
+        (G.uniform_rows(50, 3, seed=1, m=40), G.uniform_rows(70, 4, seed=2, m=50)),
+        (HostCSR(5, 50, np.zeros(6, np.int32), np.zeros(0, np.int32), np.zeros(0)),
+         G.uniform_rows(9, 2, seed=3, m=50)),
+        (G.power_law(40000, 2.0, 800, seed=4),) * 2,
+        (G.uniform_rows(300, 8, seed=5),) * 2,
+    ]
+    pairs = [(DeviceCSR.from_host(a), DeviceCSR.from_host(b)) for a, b in mats]
+    got = get_nip_many(pairs, handle)
+    assert got == [get_nip(a, b, handle) for a, b in pairs]
+    assert got == [oracle_mod.nip(a, b) for a, b in mats]
+    assert got[2] > 16384 and get_nip_many([], handle) == []
