@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--grid", type=int, default=100,
                     help="galerkin mode: points per dimension of the 27-point stencil")
     ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--no-tune", action="store_true",
+                    help="batch mode: plan the batch without the autotuner")
     ap.add_argument("--requests", type=int, default=600)
     ap.add_argument("--load", type=float, default=0.8,
                     help="served mode: offered load as a fraction of the plain path's capacity")
@@ -292,6 +294,26 @@ def run_ours(args, rank, world, local_rank):
     h.set_option(N.OPT_PROFILE, 0)
 
     value = replica_gflops(nip, args.steps, world, total_ms)
+    phase_us = h.info()["phase_us"]
+
+    # the same product planned once, its fill phase replayed as one CUDA graph
+    # (values only; the structure stays) -- reported beside the full product
+    from gpuspgemm_b200.api import plan as make_plan
+    pl = make_plan(dA, dA, handle=h)
+    for _ in range(2):
+        pl.execute()
+    rts = []
+    for _ in range(max(args.steps, 3)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        pl.execute()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        rts.append(e0.elapsed_time(e1))
+    pl.check()
+    pl.close()
+    plan_replay_ms = float(np.mean(rts))
 
     # e2e through the host-buffer entry point, pinned inputs
     pin = {k: torch.from_numpy(np.ascontiguousarray(getattr(A, k))).pin_memory()
@@ -399,7 +421,10 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": launches,
         "kernels": kernels[:12],
         "host_syncs_per_step": info["host_syncs"],
-        "host_phase_us_last_step": h.info()["phase_us"],
+        "host_phase_us_last_step": phase_us,
+        "plan_replay": {"ms": plan_replay_ms, "gflops": 2.0 * nip / (plan_replay_ms / 1e3) / 1e9,
+                        "what": "fill phase only, structure fixed: one CUDA graph launch "
+                                "(spgemm_plan_execute)"},
     }
     h.close()
     return line
@@ -449,6 +474,28 @@ def run_batch(args, local_rank):
     e1.record(stream)
     torch.cuda.synchronize()
     plain_ms = e0.elapsed_time(e1)
+    # symbolic once, numeric many: the batch planned (optionally tuned), its
+    # fill phase replayed as one CUDA graph launch per step
+    from gpuspgemm_b200.api import plan_batch
+    t0 = time.perf_counter()
+    pl = plan_batch(pb, tune=not args.no_tune, handle=h)
+    torch.cuda.synchronize()
+    plan_build_s = time.perf_counter() - t0
+    for _ in range(2):
+        pl.execute()
+    rts = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        pl.execute()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        rts.append(e0.elapsed_time(e1))
+    pl.check()
+    replay_ms = float(np.mean(rts))
+    plan_info = pl.info()
+    pl.close()
     h.close()
     return {
         "metric": "batched independent products: products/s (and GFLOPS = 2*NIP/s)",
@@ -464,6 +511,11 @@ def run_batch(args, local_rank):
         "plain_calls": {"ms_total": plain_ms, "products_per_s": pb.count / (plain_ms / 1e3),
                         "gflops": 2.0 * nip / (plain_ms / 1e3) / 1e9},
         "speedup_vs_plain_calls": plain_ms / batch_ms,
+        "plan_replay": {"ms": replay_ms, "products_per_s": pb.count / (replay_ms / 1e3),
+                        "gflops": 2.0 * nip / (replay_ms / 1e3) / 1e9,
+                        "build_s": plan_build_s, "tuning": plan_info,
+                        "what": "values recomputed for a fixed structure: one CUDA graph "
+                                "launch of every group's fill kernels and splits"},
         "clocks": clk.summary(),
     }
 

@@ -22,6 +22,8 @@ STATUS_NAMES = {
     7: "SPGEMM_ERR_INTERNAL",
 }
 
+ABI_VERSION = 2  # SPGEMM_ABI_VERSION of include/spgemm.h
+
 OPT_CHECKED = 1
 OPT_MIN_SYM_BIN = 2
 OPT_MIN_NUM_BIN = 3
@@ -66,6 +68,16 @@ class Info(C.Structure):
         ("n_num_bins", C.c_int32),
         ("host_syncs", C.c_int32),
         ("phase_us", C.c_float * 8),
+    ]
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [
+        ("candidates", C.c_int32),
+        ("chosen", C.c_int32),
+        ("team_scale", C.c_float * 8),
+        ("streams", C.c_int32 * 8),
+        ("ms", C.c_float * 8),
     ]
 
 
@@ -136,6 +148,22 @@ SIGNATURES = {
                                  C.POINTER(CsrView), C.POINTER(CsrOut), C.c_void_p]),
     "spgemm_rap_f32": (C.c_int, [C.c_void_p, C.POINTER(CsrView), C.POINTER(CsrView),
                                  C.POINTER(CsrView), C.POINTER(CsrOut), C.c_void_p]),
+    "spgemm_plan_csr_f64": (C.c_int, [C.c_void_p, C.POINTER(CsrView), C.POINTER(CsrView),
+                                      C.c_int32, C.POINTER(CsrOut), C.POINTER(C.c_void_p),
+                                      C.c_void_p]),
+    "spgemm_plan_csr_f32": (C.c_int, [C.c_void_p, C.POINTER(CsrView), C.POINTER(CsrView),
+                                      C.c_int32, C.POINTER(CsrOut), C.POINTER(C.c_void_p),
+                                      C.c_void_p]),
+    "spgemm_plan_batch_f64": (C.c_int, [C.c_void_p, C.POINTER(BatchDesc), C.POINTER(CsrView),
+                                        C.POINTER(CsrView), C.c_int32, C.POINTER(BatchOut),
+                                        C.POINTER(C.c_void_p), C.c_void_p]),
+    "spgemm_plan_batch_f32": (C.c_int, [C.c_void_p, C.POINTER(BatchDesc), C.POINTER(CsrView),
+                                        C.POINTER(CsrView), C.c_int32, C.POINTER(BatchOut),
+                                        C.POINTER(C.c_void_p), C.c_void_p]),
+    "spgemm_plan_execute": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "spgemm_plan_check": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "spgemm_plan_get_info": (C.c_int, [C.c_void_p, C.POINTER(PlanInfo)]),
+    "spgemm_plan_destroy": (C.c_int, [C.c_void_p]),
     "spgemm_row_nnz_noalloc": (C.c_int, [C.POINTER(CsrView), C.POINTER(CsrView), C.c_void_p,
                                          C.c_void_p]),
     "spgemm_last_error_string": (C.c_char_p, []),
@@ -164,7 +192,7 @@ def load(path: Path = LIB_PATH) -> C.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if lib.spgemm_abi_version() != 1:
+    if lib.spgemm_abi_version() != ABI_VERSION:
         raise ImportError("libspgemm_b200.so ABI version mismatch")
     return lib
 

@@ -300,6 +300,24 @@ def pack_batch(pairs) -> PackedBatch:
     return PackedBatch(a_row, b_row, c_col, A, B)
 
 
+def _batch_views(out: N.BatchOut, dtype) -> list[DeviceCSR]:
+    owner = _BatchOwner(out)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    vt = "<f8" if dtype == torch.float64 else "<f4"
+    res = []
+    for i in range(out.count):
+        p = out.products[i]
+        rpt = torch.as_tensor(_LibraryArray(owner, p.rpt, p.m + 1, "<i4"), device=dev)
+        if p.nnz > 0:
+            col = torch.as_tensor(_LibraryArray(owner, p.col, p.nnz, "<i4"), device=dev)
+            val = torch.as_tensor(_LibraryArray(owner, p.val, p.nnz, vt), device=dev)
+        else:
+            col = torch.empty(0, dtype=torch.int32, device=dev)
+            val = torch.empty(0, dtype=dtype, device=dev)
+        res.append(DeviceCSR(int(p.m), int(p.n), rpt, col, val))
+    return res
+
+
 def batch(pb: PackedBatch, handle: Handle | None = None, stream=None) -> list[DeviceCSR]:
     """C_i = A_i * B_i for every product of a packed batch, run as one binned
     product of the block-diagonal operands (spgemm_batch_*).  Returns one
@@ -314,21 +332,82 @@ def batch(pb: PackedBatch, handle: Handle | None = None, stream=None) -> list[De
     N.check(fn(h.ptr, C.byref(desc), C.byref(va), C.byref(vb), C.byref(out),
                _stream_ptr(stream)))
     h._last_groups = int(out.n_groups)
-    owner = _BatchOwner(out)
-    dev = torch.device("cuda", torch.cuda.current_device())
-    vt = "<f8" if pb.A.dtype == torch.float64 else "<f4"
-    res = []
-    for i in range(out.count):
-        p = out.products[i]
-        rpt = torch.as_tensor(_LibraryArray(owner, p.rpt, p.m + 1, "<i4"), device=dev)
-        if p.nnz > 0:
-            col = torch.as_tensor(_LibraryArray(owner, p.col, p.nnz, "<i4"), device=dev)
-            val = torch.as_tensor(_LibraryArray(owner, p.val, p.nnz, vt), device=dev)
-        else:
-            col = torch.empty(0, dtype=torch.int32, device=dev)
-            val = torch.empty(0, dtype=pb.A.dtype, device=dev)
-        res.append(DeviceCSR(int(p.m), int(p.n), rpt, col, val))
-    return res
+    return _batch_views(out, pb.A.dtype)
+
+
+class Plan:
+    """A product (or batch) whose structure is fixed and whose values are
+    recomputed on demand by replaying one CUDA graph (spgemm_plan_*).  Keeps
+    its operands and result alive; update A's and B's values in place, then
+    call execute()."""
+
+    def __init__(self, ptr: C.c_void_p, keep: list, result):
+        self._p = ptr
+        self._keep = keep          # operands (and packed batch) the graph reads
+        self.result = result       # DeviceCSR, or a list of them for a batch
+
+    def execute(self, stream=None) -> None:
+        N.check(N.lib().spgemm_plan_execute(self._p, _stream_ptr(stream)))
+
+    def check(self, stream=None) -> None:
+        N.check(N.lib().spgemm_plan_check(self._p, _stream_ptr(stream)))
+
+    def info(self) -> dict:
+        inf = N.PlanInfo()
+        N.check(N.lib().spgemm_plan_get_info(self._p, C.byref(inf)))
+        n = int(inf.candidates)
+        return {"candidates": [{"team_scale": round(float(inf.team_scale[i]), 3),
+                                "streams": int(inf.streams[i]), "ms": float(inf.ms[i])}
+                               for i in range(n)],
+                "chosen": int(inf.chosen)}
+
+    def close(self) -> None:
+        if self._p:
+            torch.cuda.synchronize()
+            N.lib().spgemm_plan_destroy(self._p)
+            self._p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def plan(A: DeviceCSR, B: DeviceCSR, tune: bool = False, handle: Handle | None = None,
+         stream=None) -> Plan:
+    """Plan C = A * B (spgemm_plan_csr_*): runs the product once (Plan.result)
+    and captures its fill phase for replays; tune=True picks the fastest of a
+    small grid of bin-routing and stream configurations."""
+    _require_torch()
+    if A.dtype != B.dtype:
+        raise TypeError("A and B must have the same value dtype")
+    h = handle or default_handle()
+    out = N.CsrOut()
+    p = C.c_void_p()
+    va, vb = A.view(), B.view()
+    fn = N.lib().spgemm_plan_csr_f64 if A.dtype == torch.float64 else N.lib().spgemm_plan_csr_f32
+    N.check(fn(h.ptr, C.byref(va), C.byref(vb), 1 if tune else 0, C.byref(out), C.byref(p),
+               _stream_ptr(stream)))
+    return Plan(p, [A, B], _wrap_result(out, A.dtype))
+
+
+def plan_batch(pb: PackedBatch, tune: bool = False, handle: Handle | None = None,
+               stream=None) -> Plan:
+    """Plan a packed batch (spgemm_plan_batch_*): every group's fill and split
+    become one CUDA graph; Plan.result is the list of per-product results."""
+    _require_torch()
+    h = handle or default_handle()
+    desc = N.BatchDesc(pb.count, pb.a_row_off.ctypes.data, pb.b_row_off.ctypes.data,
+                       pb.c_col_off.ctypes.data)
+    out = N.BatchOut()
+    p = C.c_void_p()
+    va, vb = pb.A.view(), pb.B.view()
+    fn = (N.lib().spgemm_plan_batch_f64 if pb.A.dtype == torch.float64
+          else N.lib().spgemm_plan_batch_f32)
+    N.check(fn(h.ptr, C.byref(desc), C.byref(va), C.byref(vb), 1 if tune else 0, C.byref(out),
+               C.byref(p), _stream_ptr(stream)))
+    return Plan(p, [pb], _batch_views(out, pb.A.dtype))
 
 
 def batch_groups(handle: Handle) -> int:

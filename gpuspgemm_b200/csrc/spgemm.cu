@@ -118,6 +118,22 @@ struct spgemm_handle_s {
     std::vector<spgemm_kernel_time> prof_done;
 };
 
+// A plan: the fill phase of one product (or of every group of a batch)
+// captured as a CUDA graph over buffers the plan owns, replayed by
+// spgemm_plan_execute to recompute C from A's and B's current values.
+struct spgemm_plan_s {
+    int device = 0;
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t capture = nullptr;       // private stream the graphs were captured on
+    cudaGraph_t graph = nullptr;          // the whole plan (a parent graph for batches)
+    std::vector<cudaGraph_t> children;    // per-group graphs of a batch plan
+    cudaGraphExec_t exec = nullptr;
+    b200::DevStatus* status = nullptr;    // written by the captured kernels
+    b200::DevStatus* status_host = nullptr;  // pinned
+    std::vector<void*> owned;             // device buffers the graph reads
+    spgemm_plan_info info = {};
+};
+
 namespace b200 {
 namespace {
 
@@ -324,9 +340,42 @@ spgemm_status launch_bins(spgemm_handle_s* h, const BinLauncher* bins, int nb, i
     return join_streams(h, main);
 }
 
+// Plan capture request for product(): the team fill bins' routing limits are
+// scaled by team_scale (rows above the scaled limit go to the next, wider
+// bin; a tuning knob), and with `plan` set the fill launches are captured as
+// a graph over plan-owned copies of the bin lists, bitmaps and status word.
+// launch_now: instantiate the graph into plan->exec and run it (single
+// products); otherwise hand it back in `graph` (batch groups).
+struct CaptureReq {
+    double team_scale = 1.0;
+    spgemm_plan_s* plan = nullptr;
+    bool launch_now = true;
+    cudaGraph_t graph = nullptr;
+};
+
+Ladder scaled_ladder(const BinLauncher* bins, int nb, int min_bin, double team_scale) {
+    Ladder l = make_ladder(bins, nb, min_bin);
+    if (team_scale >= 1.0) return l;
+    int prev = 0;
+    for (int i = 0; i < nb; i++) {
+        if (bins[i].kind == BinKind::Team) {
+            const int lim = static_cast<int>(bins[i].limit * team_scale);
+            l.limit[i] = lim > prev ? lim : prev + 1;  // limits stay increasing
+        }
+        prev = l.limit[i];
+    }
+    return l;
+}
+
+spgemm_status plan_alloc(spgemm_plan_s* plan, void** p, size_t bytes, cudaStream_t stream) {
+    B200_TRY(cudaMallocFromPoolAsync(p, bytes, plan->pool, stream));
+    plan->owned.push_back(*p);
+    return SPGEMM_OK;
+}
+
 template<typename V>
 spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm_csr_view* B,
-                      spgemm_csr_out* C, cudaStream_t stream) {
+                      spgemm_csr_out* C, cudaStream_t stream, CaptureReq* cr = nullptr) {
     if (h == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "handle is NULL");
     if (C == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "C is NULL");
     if (spgemm_status st = check_view(A, "A"); st != SPGEMM_OK) return st;
@@ -500,7 +549,7 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     B200_STEP(join_streams(h, stream));
 
     // ---- scan pass: row pointer and fill bins -------------------------------
-    const Ladder lad2 = make_ladder(fil, nfil, h->min_num_bin);
+    const Ladder lad2 = scaled_ladder(fil, nfil, h->min_num_bin, cr ? cr->team_scale : 1.0);
     B200_STEP(timed(h, "nnz_hist", 2, -1, m, stream, [&](cudaStream_t ss) {
         return launch_nnz_hist(c_rpt, m, s.hist2, s.cta_sum, s.plan2, lad2, ss);
     }));
@@ -550,9 +599,54 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         pa.nmaps = nmaps;
     }
     mark(4);
-    B200_STEP(launch_bins(h, fil, nfil, 3, p2, s.bins2, pa, stream));
+    DevStatus* fill_status = s.status;
+    if (cr != nullptr && cr->plan != nullptr) {
+        // the graph reads copies the plan owns: later products reuse the
+        // handle's scratch and bitmaps
+        spgemm_plan_s* plan = cr->plan;
+        int32_t* bins = nullptr;
+        B200_STEP(plan_alloc(plan, reinterpret_cast<void**>(&bins), sizeof(int32_t) * size_t(m),
+                             stream));
+        if (cudaError_t e = cudaMemcpyAsync(bins, s.bins2, sizeof(int32_t) * size_t(m),
+                                            cudaMemcpyDeviceToDevice, stream);
+            e != cudaSuccess)
+            return bail(cuda_fail(e, "copy fill bins"));
+        if (pa.bitmaps != nullptr) {
+            void* bm = nullptr;
+            B200_STEP(plan_alloc(plan, &bm, sizeof(uint32_t) * size_t(pa.words) * size_t(pa.nmaps),
+                                 stream));
+            pa.bitmaps = static_cast<uint32_t*>(bm);
+        }
+        pa.status = plan->status;
+        fill_status = plan->status;
+        const int saved_profile = h->profile;
+        h->profile = 0;
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(plan->capture, cudaStreamCaptureModeThreadLocal);
+        spgemm_status st = e == cudaSuccess
+                               ? launch_bins(h, fil, nfil, 3, p2, bins, pa, plan->capture)
+                               : cuda_fail(e, "begin capture");
+        const cudaError_t ee = cudaStreamEndCapture(plan->capture, &g);
+        h->profile = saved_profile;
+        if (st != SPGEMM_OK) {
+            if (g) cudaGraphDestroy(g);
+            return bail(st);
+        }
+        if (ee != cudaSuccess) return bail(cuda_fail(ee, "end capture"));
+        if (cr->launch_now) {
+            plan->graph = g;
+            if (cudaError_t e2 = cudaGraphInstantiate(&plan->exec, g, 0); e2 != cudaSuccess)
+                return bail(cuda_fail(e2, "instantiate the fill graph"));
+            if (cudaError_t e2 = cudaGraphLaunch(plan->exec, stream); e2 != cudaSuccess)
+                return bail(cuda_fail(e2, "launch the fill graph"));
+        } else {
+            cr->graph = g;
+        }
+    } else {
+        B200_STEP(launch_bins(h, fil, nfil, 3, p2, s.bins2, pa, stream));
+    }
     mark(5);
-    if (cudaError_t e = cudaMemcpyAsync(&h->mirror->status, s.status, sizeof(DevStatus),
+    if (cudaError_t e = cudaMemcpyAsync(&h->mirror->status, fill_status, sizeof(DevStatus),
                                         cudaMemcpyDeviceToHost, stream);
         e != cudaSuccess)
         return bail(cuda_fail(e, "read status"));
@@ -575,7 +669,8 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
 // column indices, as views into the group's arrays.
 template<typename V>
 spgemm_status batch(spgemm_handle_s* h, const spgemm_batch_desc* d, const spgemm_csr_view* A,
-                    const spgemm_csr_view* B, spgemm_batch_out* out, cudaStream_t stream) {
+                    const spgemm_csr_view* B, spgemm_batch_out* out, cudaStream_t stream,
+                    spgemm_plan_s* plan = nullptr, double team_scale = 1.0) {
     if (h == nullptr || d == nullptr || out == nullptr)
         return fail(SPGEMM_ERR_INVALID_ARG, "NULL argument");
     std::memset(out, 0, sizeof(*out));
@@ -615,7 +710,11 @@ spgemm_status batch(spgemm_handle_s* h, const spgemm_batch_desc* d, const spgemm
     const size_t total = align_up(o_pos + nb_pos, 256);
     char* dbuf = nullptr;
     B200_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&dbuf), total, h->pool, stream));
-    auto release = [&]() { cudaFreeAsync(dbuf, stream); };
+    // a plan's graph reads the offsets and writes the positions at every run
+    auto release = [&]() {
+        if (plan == nullptr) cudaFreeAsync(dbuf, stream);
+    };
+    if (plan != nullptr) plan->owned.push_back(dbuf);
     int32_t* d_row = reinterpret_cast<int32_t*>(dbuf + o_row);
     int32_t* d_col = reinterpret_cast<int32_t*>(dbuf + o_col);
     int64_t* d_off = reinterpret_cast<int64_t*>(dbuf + o_off);
@@ -676,6 +775,7 @@ spgemm_status batch(spgemm_handle_s* h, const spgemm_batch_desc* d, const spgemm
 
     constexpr long long kGroupLimit = INT32_MAX;
     int32_t groups = 0;
+    std::vector<std::pair<cudaGraph_t, cudaGraph_t>> group_graphs;  // plan: (fill, split)
     spgemm_info acc = {};
     for (int p0 = 0; p0 < count;) {
         long long sum = 0;
@@ -687,7 +787,11 @@ spgemm_status batch(spgemm_handle_s* h, const spgemm_batch_desc* d, const spgemm
         Ag.m = r1 - r0;
         Ag.rpt = A->rpt + r0;
         spgemm_csr_out Cg;
-        spgemm_status st = product<V>(h, &Ag, B, &Cg, stream);
+        CaptureReq cr;
+        cr.team_scale = team_scale;
+        cr.plan = plan;
+        cr.launch_now = false;
+        spgemm_status st = product<V>(h, &Ag, B, &Cg, stream, &cr);
         if (st != SPGEMM_OK) {
             h->checked = saved_checked;
             return unwind(st);
@@ -704,9 +808,29 @@ spgemm_status batch(spgemm_handle_s* h, const spgemm_batch_desc* d, const spgemm
         }
         if (Cg.col) blocks.push_back(Cg.col);
         if (Cg.val) blocks.push_back(Cg.val);
-        e = launch_unpack(Cg.rpt, Cg.col, d_row, d_col, d_off, p0, p1 - p0, rpt_out, d_pos,
-                          stream);
-        if (e == cudaSuccess) e = cudaFreeAsync(Cg.rpt, stream);  // split copies what it needs
+        if (plan == nullptr) {
+            e = launch_unpack(Cg.rpt, Cg.col, d_row, d_col, d_off, p0, p1 - p0, rpt_out, d_pos,
+                              stream);
+            if (e == cudaSuccess) e = cudaFreeAsync(Cg.rpt, stream);  // split copies what it needs
+        } else {
+            // the group's fill graph, then its split, as two nodes of the plan
+            plan->owned.push_back(Cg.rpt);  // the split reads it at every run
+            cudaGraph_t split = nullptr;
+            e = cudaStreamBeginCapture(plan->capture, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess)
+                e = launch_unpack(Cg.rpt, Cg.col, d_row, d_col, d_off, p0, p1 - p0, rpt_out,
+                                  d_pos, plan->capture);
+            const cudaError_t ee = cudaStreamEndCapture(plan->capture, &split);
+            if (e == cudaSuccess) e = ee;
+            if (e == cudaSuccess) {
+                group_graphs.emplace_back(cr.graph, split);  // no fill graph when nnz = 0
+                if (cr.graph) plan->children.push_back(cr.graph);
+                plan->children.push_back(split);
+            } else {
+                if (cr.graph) cudaGraphDestroy(cr.graph);
+                if (split) cudaGraphDestroy(split);
+            }
+        }
         if (e != cudaSuccess) {
             h->checked = saved_checked;
             return unwind(cuda_fail(e, "batch split"));
@@ -721,6 +845,23 @@ spgemm_status batch(spgemm_handle_s* h, const spgemm_batch_desc* d, const spgemm
         p0 = p1;
     }
     h->checked = saved_checked;
+    if (plan != nullptr) {
+        // one parent graph: per group, fill then split; groups are independent
+        e = cudaGraphCreate(&plan->graph, 0);
+        for (size_t i = 0; e == cudaSuccess && i < group_graphs.size(); i++) {
+            cudaGraphNode_t fill = nullptr;
+            cudaGraphNode_t split = nullptr;
+            if (group_graphs[i].first != nullptr)
+                e = cudaGraphAddChildGraphNode(&fill, plan->graph, nullptr, 0,
+                                               group_graphs[i].first);
+            if (e == cudaSuccess)
+                e = cudaGraphAddChildGraphNode(&split, plan->graph, fill ? &fill : nullptr,
+                                               fill ? 1 : 0, group_graphs[i].second);
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&plan->exec, plan->graph, 0);
+        if (e == cudaSuccess) e = cudaGraphLaunch(plan->exec, stream);
+        if (e != cudaSuccess) return unwind(cuda_fail(e, "batch plan graph"));
+    }
     std::vector<int32_t> pos(2 * size_t(count));
     e = cudaMemcpyAsync(pos.data(), d_pos, nb_pos, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
@@ -1062,6 +1203,131 @@ spgemm_status rap(spgemm_handle_s* h, const spgemm_csr_view* R, const spgemm_csr
     return SPGEMM_OK;
 }
 
+// ---- plans: the fill phase as a replayable CUDA graph -------------------------
+
+spgemm_status plan_new(spgemm_handle_s* h, spgemm_plan_s** out, cudaStream_t stream) {
+    auto* p = new spgemm_plan_s();
+    p->device = h->device;
+    p->pool = h->pool;
+    *out = p;
+    B200_TRY(cudaStreamCreateWithFlags(&p->capture, cudaStreamNonBlocking));
+    B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&p->status_host), sizeof(DevStatus)));
+    B200_TRY(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p->status), sizeof(DevStatus),
+                                     p->pool, stream));
+    p->owned.push_back(p->status);
+    B200_TRY(cudaMemsetAsync(p->status, 0, sizeof(DevStatus), stream));
+    return SPGEMM_OK;
+}
+
+// The caller has synchronised every stream the plan ran on.
+void plan_free(spgemm_plan_s* p) {
+    if (p == nullptr) return;
+    cudaSetDevice(p->device);
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    for (cudaGraph_t g : p->children)
+        if (g) cudaGraphDestroy(g);
+    for (void* b : p->owned) cudaFreeAsync(b, p->capture);
+    if (p->capture) {
+        cudaStreamSynchronize(p->capture);
+        cudaStreamDestroy(p->capture);
+    }
+    if (p->status_host) cudaFreeHost(p->status_host);
+    delete p;
+}
+
+// Median of three timed replays (after one warm replay) on `stream`.
+spgemm_status plan_time(spgemm_plan_s* p, cudaStream_t stream, float* ms) {
+    *ms = 0.0f;
+    if (p->exec == nullptr) return SPGEMM_OK;  // nothing to fill (nnz(C) = 0)
+    cudaEvent_t a, b;
+    B200_TRY(cudaEventCreate(&a));
+    B200_TRY(cudaEventCreate(&b));
+    float t[3] = {};
+    cudaError_t e = cudaGraphLaunch(p->exec, stream);
+    for (int i = 0; e == cudaSuccess && i < 3; i++) {
+        e = cudaEventRecord(a, stream);
+        if (e == cudaSuccess) e = cudaGraphLaunch(p->exec, stream);
+        if (e == cudaSuccess) e = cudaEventRecord(b, stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t[i], a, b);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (e != cudaSuccess) return cuda_fail(e, "time a plan");
+    std::sort(t, t + 3);
+    *ms = t[1];
+    return SPGEMM_OK;
+}
+
+// Build a plan with `make(plan, team_scale)` -- a product or a batch in plan
+// mode, which also fills the caller's output -- once with the default
+// configuration, or, when tuning, once per candidate (team bins' routing
+// scale x side streams), keeping the fastest replay.  `drop` frees the output
+// of a candidate that loses.
+template<typename Make, typename Drop>
+spgemm_status plan_build(spgemm_handle_s* h, int tune, cudaStream_t stream, Make&& make,
+                         Drop&& drop, spgemm_plan_s** out) {
+    static constexpr double kScales[] = {1.0, 0.75, 0.5};
+    static constexpr int kStreams[] = {4, 8};
+    struct Cand {
+        double scale;
+        int streams;
+    };
+    std::vector<Cand> cands;
+    if (tune) {
+        for (double sc : kScales)
+            for (int ns : kStreams) cands.push_back({sc, ns});
+    } else {
+        cands.push_back({1.0, h->nside});
+    }
+    const int saved_nside = h->nside;
+    spgemm_plan_s* best = nullptr;
+    int best_i = -1;
+    spgemm_plan_info info = {};
+    info.candidates = static_cast<int32_t>(cands.size());
+    spgemm_status st = SPGEMM_OK;
+    for (size_t i = 0; i < cands.size() && st == SPGEMM_OK; i++) {
+        h->nside = cands[i].streams;
+        spgemm_plan_s* p = nullptr;
+        st = plan_new(h, &p, stream);
+        if (st == SPGEMM_OK) st = make(p, cands[i].scale);
+        float ms = 0.0f;
+        if (st == SPGEMM_OK) st = plan_time(p, stream, &ms);
+        if (st != SPGEMM_OK) {
+            cudaStreamSynchronize(stream);
+            plan_free(p);
+            break;
+        }
+        info.team_scale[i] = static_cast<float>(cands[i].scale);
+        info.streams[i] = cands[i].streams;
+        info.ms[i] = ms;
+        if (best == nullptr || ms < info.ms[best_i]) {
+            if (best != nullptr) {
+                drop(true);  // the previous best's output
+                plan_free(best);
+            }
+            best = p;
+            best_i = static_cast<int>(i);
+        } else {
+            drop(false);  // this candidate's output
+            plan_free(p);
+        }
+    }
+    h->nside = saved_nside;
+    if (st != SPGEMM_OK) {
+        if (best != nullptr) {
+            drop(true);
+            plan_free(best);
+        }
+        return st;
+    }
+    info.chosen = best_i;
+    best->info = info;
+    *out = best;
+    return SPGEMM_OK;
+}
+
 // One stream-ordered memory pool per device for every handle's results,
 // created on first use and never destroyed: results may outlive the handle
 // that made them, and a pool must not go away under live allocations.  Its
@@ -1095,6 +1361,77 @@ spgemm_status device_pool(int dev, cudaMemPool_t* out) {
     }
     g_pool_users[dev]++;
     *out = g_pools[dev];
+    return SPGEMM_OK;
+}
+
+template<typename V>
+spgemm_status plan_csr(spgemm_handle_t h, const spgemm_csr_view* A, const spgemm_csr_view* B,
+                       int32_t tune, spgemm_csr_out* C, spgemm_plan_t* plan, void* stream) {
+    if (h == nullptr || C == nullptr || plan == nullptr)
+        return fail(SPGEMM_ERR_INVALID_ARG, "NULL argument");
+    *plan = nullptr;
+    std::memset(C, 0, sizeof(*C));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    B200_TRY(cudaSetDevice(h->device));
+    // the kept plan's output is in *C; a losing candidate's output is freed
+    spgemm_csr_out cur = {};
+    auto make = [&](spgemm_plan_s* p, double scale) {
+        CaptureReq cr;
+        cr.team_scale = scale;
+        cr.plan = p;
+        cr.launch_now = true;
+        return product<V>(h, A, B, &cur, s, &cr);
+    };
+    auto drop = [&](bool previous_best) {
+        if (previous_best) {
+            spgemm_csr_free(C, s);
+            *C = cur;
+        } else {
+            spgemm_csr_free(&cur, s);
+        }
+    };
+    spgemm_plan_s* p = nullptr;
+    // plan_build calls make() then drop(); the first candidate becomes the best
+    // without a drop, so move its output into *C right after
+    auto make_first = [&](spgemm_plan_s* pl, double scale) {
+        const spgemm_status st = make(pl, scale);
+        if (st == SPGEMM_OK && C->rpt == nullptr) *C = cur;
+        return st;
+    };
+    const spgemm_status st = plan_build(h, tune, s, make_first, drop, &p);
+    if (st != SPGEMM_OK) return st;
+    *plan = p;
+    return SPGEMM_OK;
+}
+
+template<typename V>
+spgemm_status plan_batch(spgemm_handle_t h, const spgemm_batch_desc* d, const spgemm_csr_view* A,
+                         const spgemm_csr_view* B, int32_t tune, spgemm_batch_out* out,
+                         spgemm_plan_t* plan, void* stream) {
+    if (h == nullptr || out == nullptr || plan == nullptr)
+        return fail(SPGEMM_ERR_INVALID_ARG, "NULL argument");
+    *plan = nullptr;
+    std::memset(out, 0, sizeof(*out));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    B200_TRY(cudaSetDevice(h->device));
+    spgemm_batch_out cur = {};
+    auto make = [&](spgemm_plan_s* p, double scale) {
+        const spgemm_status st = batch<V>(h, d, A, B, &cur, s, p, scale);
+        if (st == SPGEMM_OK && out->products == nullptr) *out = cur;
+        return st;
+    };
+    auto drop = [&](bool previous_best) {
+        if (previous_best) {
+            spgemm_batch_free(out, s);
+            *out = cur;
+        } else {
+            spgemm_batch_free(&cur, s);
+        }
+    };
+    spgemm_plan_s* p = nullptr;
+    const spgemm_status st = plan_build(h, tune, s, make, drop, &p);
+    if (st != SPGEMM_OK) return st;
+    *plan = p;
     return SPGEMM_OK;
 }
 
@@ -1218,6 +1555,62 @@ spgemm_status spgemm_rap_f32(spgemm_handle_t h, const spgemm_csr_view* R,
                              const spgemm_csr_view* A, const spgemm_csr_view* P,
                              spgemm_csr_out* C, void* stream) {
     return rap<float>(h, R, A, P, C, static_cast<cudaStream_t>(stream));
+}
+
+spgemm_status spgemm_plan_csr_f64(spgemm_handle_t h, const spgemm_csr_view* A,
+                                  const spgemm_csr_view* B, int32_t tune, spgemm_csr_out* C,
+                                  spgemm_plan_t* plan, void* stream) {
+    return plan_csr<double>(h, A, B, tune, C, plan, stream);
+}
+
+spgemm_status spgemm_plan_csr_f32(spgemm_handle_t h, const spgemm_csr_view* A,
+                                  const spgemm_csr_view* B, int32_t tune, spgemm_csr_out* C,
+                                  spgemm_plan_t* plan, void* stream) {
+    return plan_csr<float>(h, A, B, tune, C, plan, stream);
+}
+
+spgemm_status spgemm_plan_batch_f64(spgemm_handle_t h, const spgemm_batch_desc* d,
+                                    const spgemm_csr_view* A, const spgemm_csr_view* B,
+                                    int32_t tune, spgemm_batch_out* out, spgemm_plan_t* plan,
+                                    void* stream) {
+    return plan_batch<double>(h, d, A, B, tune, out, plan, stream);
+}
+
+spgemm_status spgemm_plan_batch_f32(spgemm_handle_t h, const spgemm_batch_desc* d,
+                                    const spgemm_csr_view* A, const spgemm_csr_view* B,
+                                    int32_t tune, spgemm_batch_out* out, spgemm_plan_t* plan,
+                                    void* stream) {
+    return plan_batch<float>(h, d, A, B, tune, out, plan, stream);
+}
+
+spgemm_status spgemm_plan_execute(spgemm_plan_t plan, void* stream) {
+    if (plan == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "plan is NULL");
+    if (plan->exec == nullptr) return SPGEMM_OK;  // C has no entries to recompute
+    B200_TRY(cudaSetDevice(plan->device));
+    B200_TRY(cudaGraphLaunch(plan->exec, static_cast<cudaStream_t>(stream)));
+    return SPGEMM_OK;
+}
+
+spgemm_status spgemm_plan_check(spgemm_plan_t plan, void* stream) {
+    if (plan == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "plan is NULL");
+    B200_TRY(cudaSetDevice(plan->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    B200_TRY(cudaMemcpyAsync(plan->status_host, plan->status, sizeof(DevStatus),
+                             cudaMemcpyDeviceToHost, s));
+    B200_TRY(cudaMemsetAsync(plan->status, 0, sizeof(DevStatus), s));
+    B200_TRY(cudaStreamSynchronize(s));
+    return status_to_error(*plan->status_host);
+}
+
+spgemm_status spgemm_plan_get_info(spgemm_plan_t plan, spgemm_plan_info* info) {
+    if (plan == nullptr || info == nullptr) return fail(SPGEMM_ERR_INVALID_ARG, "NULL argument");
+    *info = plan->info;
+    return SPGEMM_OK;
+}
+
+spgemm_status spgemm_plan_destroy(spgemm_plan_t plan) {
+    plan_free(plan);
+    return SPGEMM_OK;
 }
 
 spgemm_status spgemm_batch_f64(spgemm_handle_t h, const spgemm_batch_desc* d,

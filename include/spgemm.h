@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define SPGEMM_ABI_VERSION 1
+#define SPGEMM_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define SPGEMM_API __attribute__((visibility("default")))
@@ -275,6 +275,64 @@ SPGEMM_API spgemm_status spgemm_batch_f32(spgemm_handle_t handle, const spgemm_b
                                           const spgemm_csr_view* A, const spgemm_csr_view* B,
                                           spgemm_batch_out* out, void* stream);
 SPGEMM_API spgemm_status spgemm_batch_free(spgemm_batch_out* out, void* stream);
+
+/* ---- plans: symbolic once, numeric many ------------------------------------ */
+
+/* A plan fixes C's structure and the fill phase's bins for operands whose
+ * STRUCTURE stays the same while their VALUES change (same device arrays,
+ * updated in place): iterative solvers, AMG setup with new coefficients, a
+ * batch of the same products every step.  Creating it runs the whole product
+ * once (C is returned as from spgemm_csr_* / spgemm_batch_*) and captures the
+ * fill kernels -- every bin of every group, side-stream branches included --
+ * as ONE CUDA graph.  spgemm_plan_execute replays it: C's values (and, again,
+ * its sorted columns) are recomputed from A's and B's current values with one
+ * graph launch and no host synchronisation.
+ *
+ * tune = 1 runs an autotuner first: it builds the plan for every candidate of
+ * a small grid -- the team fill bins' routing limits scaled by 1, 0.75 or 0.5
+ * (rows above a scaled limit go to the next, wider bin) times 4 or 8 side
+ * streams (parallel branches of the graph) -- times three replays of each and
+ * keeps the fastest (spgemm_plan_get_info reports all of them).  tune = 0
+ * keeps the default ladder.
+ *
+ * A, B, C (and a batch's blocks) must stay allocated while the plan lives;
+ * destroy the plan after its last execution has completed.  No counterpart in
+ * the reference, which recomputes the structure on every call. */
+typedef struct spgemm_plan_s* spgemm_plan_t;
+
+typedef struct spgemm_plan_info {
+    int32_t candidates;   /* configurations built (1 without tuning) */
+    int32_t chosen;       /* index of the one the plan keeps */
+    float team_scale[8];  /* routing limits of the team fill bins x this */
+    int32_t streams[8];   /* side streams = parallel branches of the graph */
+    float ms[8];          /* median replay time of each configuration */
+} spgemm_plan_info;
+
+SPGEMM_API spgemm_status spgemm_plan_csr_f64(spgemm_handle_t handle, const spgemm_csr_view* A,
+                                             const spgemm_csr_view* B, int32_t tune,
+                                             spgemm_csr_out* C, spgemm_plan_t* plan,
+                                             void* stream);
+SPGEMM_API spgemm_status spgemm_plan_csr_f32(spgemm_handle_t handle, const spgemm_csr_view* A,
+                                             const spgemm_csr_view* B, int32_t tune,
+                                             spgemm_csr_out* C, spgemm_plan_t* plan,
+                                             void* stream);
+SPGEMM_API spgemm_status spgemm_plan_batch_f64(spgemm_handle_t handle,
+                                               const spgemm_batch_desc* desc,
+                                               const spgemm_csr_view* A, const spgemm_csr_view* B,
+                                               int32_t tune, spgemm_batch_out* out,
+                                               spgemm_plan_t* plan, void* stream);
+SPGEMM_API spgemm_status spgemm_plan_batch_f32(spgemm_handle_t handle,
+                                               const spgemm_batch_desc* desc,
+                                               const spgemm_csr_view* A, const spgemm_csr_view* B,
+                                               int32_t tune, spgemm_batch_out* out,
+                                               spgemm_plan_t* plan, void* stream);
+/* Replay: asynchronous on `stream` (one graph launch). */
+SPGEMM_API spgemm_status spgemm_plan_execute(spgemm_plan_t plan, void* stream);
+/* Synchronise `stream` and report device-side errors of the executions since
+ * the last check (capacity or probe-bound flags, as for a product). */
+SPGEMM_API spgemm_status spgemm_plan_check(spgemm_plan_t plan, void* stream);
+SPGEMM_API spgemm_status spgemm_plan_get_info(spgemm_plan_t plan, spgemm_plan_info* info);
+SPGEMM_API spgemm_status spgemm_plan_destroy(spgemm_plan_t plan);
 
 /* ---- allocation-free row sizes --------------------------------------------- */
 
