@@ -39,7 +39,7 @@ def build(ref: bool | None = None) -> None:
     if ref is None:
         ref = REF_SRC.exists()
     if ref:
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref",
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", "opsparse",
                         f"PYTHON={sys.executable}"], check=True)
 
 
@@ -253,3 +253,67 @@ def ref_time(which: str, A: HostCSR, B: HostCSR, dtype=None, warmups: int = 3,
         raise RuntimeError(ref_lib().ref_last_error().decode())
     del keep
     return list(secs), int(nipv[0])
+
+
+# ---- the reference's vendored OpSparse (oracle/_ref/libref_opsparse_*.so) ----
+
+OPS_LIBS = {np.dtype(np.float64): HERE / "_ref" / "libref_opsparse_f64.so",
+            np.dtype(np.float32): HERE / "_ref" / "libref_opsparse_f32.so"}
+_ops = {}
+
+
+def ops_available(dtype=np.float64) -> bool:
+    return OPS_LIBS[np.dtype(dtype)].exists()
+
+
+def ops_lib(dtype=np.float64) -> C.CDLL:
+    dtype = np.dtype(dtype)
+    if dtype not in _ops:
+        path = OPS_LIBS[dtype]
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (make -C oracle opsparse)")
+        l = C.CDLL(str(path))
+        args = [C.c_int32, C.c_int32, C.c_int32, _P, _P, _P] * 2
+        l.ops_run.restype = C.c_int
+        l.ops_run.argtypes = args + [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]
+        l.ops_time.restype = C.c_int
+        l.ops_time.argtypes = args + [C.c_int, C.c_int, _P]
+        l.ops_last_error.restype = C.c_char_p
+        l.ops_free.argtypes = [_P]
+        assert l.ops_value_bytes() == dtype.itemsize
+        _ops[dtype] = l
+    return _ops[dtype]
+
+
+def ops_run(A: HostCSR, B: HostCSR, dtype=np.float64) -> HostCSR:
+    """C = A * B through the reference's vendored OpSparse (src/libopsparse)."""
+    dtype = np.dtype(dtype)
+    l = ops_lib(dtype)
+    args, keep = _ref_args(A, B, dtype)
+    dims = np.zeros(3, dtype=np.int32)
+    prpt, pcol, pval = _P(), _P(), _P()
+    if l.ops_run(*args, _p(dims), C.byref(prpt), C.byref(pcol), C.byref(pval)) != 0:
+        raise RuntimeError(l.ops_last_error().decode())
+    m, n, nnz = (int(x) for x in dims)
+    ct = C.c_double if dtype == np.float64 else C.c_float
+    rpt = np.ctypeslib.as_array(C.cast(prpt, C.POINTER(C.c_int32)), (m + 1,)).copy()
+    col = np.ctypeslib.as_array(C.cast(pcol, C.POINTER(C.c_int32)), (max(nnz, 1),))[:nnz].copy()
+    val = np.ctypeslib.as_array(C.cast(pval, C.POINTER(ct)), (max(nnz, 1),))[:nnz].copy()
+    for q in (prpt, pcol, pval):
+        l.ops_free(q)
+    del keep
+    return HostCSR(m, n, rpt, col, val)
+
+
+def ops_time(A: HostCSR, B: HostCSR, dtype=np.float64, warmups: int = 3,
+             runs: int = 5) -> list[float]:
+    """Wall-clock seconds per OpSparse call, as the reference's opsparse app
+    measures them (src/apps/opsparse.cu:35-44)."""
+    dtype = np.dtype(dtype)
+    l = ops_lib(dtype)
+    args, keep = _ref_args(A, B, dtype)
+    secs = np.zeros(runs, dtype=np.float64)
+    if l.ops_time(*args, warmups, runs, _p(secs)) != 0:
+        raise RuntimeError(l.ops_last_error().decode())
+    del keep
+    return list(secs)

@@ -12,7 +12,8 @@
 //     the reference's `validate` oracle (src/apps/common.hpp:116-120).
 //   - utils::get_nip (src/libutils/include/utils/nip.cuh:52-78).
 // Timing follows the reference's `measure` lambda (src/apps/proposal.cu:28-35):
-// steady_clock around the call plus cudaDeviceSynchronize, C freed inside.
+// steady_clock around the call plus cudaDeviceSynchronize; C is freed after
+// the clock stops.
 //
 // Nothing here is part of the product; the product library never links it.
 
@@ -92,16 +93,22 @@ int time_calls(int which, int32_t am, int32_t an, int32_t annz, const int32_t* a
         const auto hb = make_host<T>(bm, bn, bnnz, brpt, bcol, bval);
         const auto da = ha.template to<utils::Location::Device>();
         const auto db = hb.template to<utils::Location::Device>();
+        // the clock stops before C is destroyed, as in the app's measure
+        // lambda, where C lives until the lambda returns
         auto once = [&]() -> double {
-            const auto t0 = Clock::now();
+            Clock::time_point t0;
+            Clock::time_point t1;
             if (which == 0) {
+                t0 = Clock::now();
                 auto c = proposal::proposal_inner<T, proposal::Parameters<proposal::CC80>>(da, db);
                 utils::device_sync();
+                t1 = Clock::now();
             } else {
+                t0 = Clock::now();
                 auto c = cusparse2<T>(da, db);
                 utils::device_sync();
+                t1 = Clock::now();
             }
-            const auto t1 = Clock::now();
             return std::chrono::duration<double>(t1 - t0).count();
         };
         for (int i = 0; i < warmups; i++) once();
