@@ -38,13 +38,20 @@ METRIC = "C=A*A GFLOPS (2*NIP/s), power-law n=1e6 FP64"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic
-# byte of a fill kernel, from one ncu capture of the power-law n = 200,000
-# case (profiles/s2n_fused_powerlaw200k_f64.md: 10.84 MB read + 0.008 MB
-# written against 20.80 MB algorithmic for the same launch).  The capture is
-# scaled to the launch the bench reports by its algorithmic bytes: at both
-# sizes A and B fit in L2, so DRAM reads are the first touch of A's and B's
-# rows and C's writes drain from L2 after the kernel.
-TRAFFIC_PER_ALG_BYTE = {"s2n_team32_t1024": (10844160 + 7680) / 20804236}
+# byte of the fill kernels, from one ncu capture of the power-law n = 200,000
+# case (profiles/s2n_fused_powerlaw200k_f64.md; ncu runs each launch from cold
+# caches): the kernel's DRAM bytes over the algorithmic bytes of the same
+# launch, as this bench computes them for that case.  The bench scales the
+# ratio to the launch it reports by that launch's algorithmic bytes: at both
+# sizes A and B fit in L2, so DRAM reads are the first touch of the A and B
+# rows a bin reads, and C's writes drain from L2 after the kernel.
+TRAFFIC_PER_ALG_BYTE = {
+    "s2n_team4_t16": 11508224 / 14947704,
+    "s2n_team8_t64": 10017792 / 11855028,
+    "s2n_team16_t256": 10184960 / 16517676,
+    "s2n_team32_t1024": 10851840 / 20804236,
+    "s2n_cta256_t4096": 11505152 / 24898604,
+}
 
 
 def parse():

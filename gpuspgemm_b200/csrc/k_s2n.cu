@@ -134,17 +134,19 @@ __global__ __launch_bounds__(THREADS) void k_s2n_cta(ProductArgs p) {
 // columns).  atomicOr fills it; the set bits read in word order are the sorted
 // column list, so no sort is needed.  Extraction: each warp owns a contiguous
 // run of words; warp totals are scanned across the CTA, then each warp scans
-// its 32-word chunks with shuffles and writes its columns.  The bitmap's space
-// then holds the row's values for the binary-search accumulation.
+// its 32-word chunks with shuffles, writes its columns to C.col and records
+// the rank of every 8-word block's first bit.  The bitmap stays intact, so a
+// key's position in the row is its rank -- the block's rank plus the set bits
+// before it in at most 8 words, all independent reads -- instead of a binary
+// search; values accumulate with global reductions into C.val.  Shared memory
+// does not grow with the row, so every row of the bin's range fits.
 constexpr int kBitmapWords = kBitmapCols / 32;
 
 template<typename V, int THREADS, int CAP>
 struct BitmapLayout {
     static constexpr size_t bm_bytes = sizeof(uint32_t) * kBitmapWords;
-    static constexpr size_t region0 =
-        bm_bytes > sizeof(V) * CAP ? bm_bytes : sizeof(V) * CAP;
-    static constexpr size_t cols_bytes = sizeof(int32_t) * CAP;
-    static constexpr size_t bytes = region0 + cols_bytes + sizeof(CtaScratch<THREADS>);
+    static constexpr size_t rank_bytes = sizeof(int32_t) * (kBitmapWords / 8);
+    static constexpr size_t bytes = bm_bytes + rank_bytes + sizeof(CtaScratch<THREADS>);
 };
 
 template<typename V, int THREADS, int CAP>
@@ -153,9 +155,8 @@ __global__ __launch_bounds__(THREADS) void k_s2n_bitmap(ProductArgs p) {
     constexpr int NW = THREADS / kWarp;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* bm = reinterpret_cast<uint32_t*>(smem_raw);
-    V* vals = reinterpret_cast<V*>(smem_raw);  // after the bitmap is read out
-    int32_t* cols = reinterpret_cast<int32_t*>(smem_raw + L::region0);
-    auto& sc = *reinterpret_cast<CtaScratch<THREADS>*>(smem_raw + L::region0 + L::cols_bytes);
+    int32_t* block_rank = reinterpret_cast<int32_t*>(smem_raw + L::bm_bytes);
+    auto& sc = *reinterpret_cast<CtaScratch<THREADS>*>(smem_raw + L::bm_bytes + L::rank_bytes);
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int w = tid >> 5;
@@ -193,6 +194,7 @@ __global__ __launch_bounds__(THREADS) void k_s2n_bitmap(ProductArgs p) {
         base += k < w ? t : 0;
         total += t;
     }
+    int32_t* cols = p.c_col + c0;
     for (int c = w0; c < w1; c += kWarp) {
         const int i = c + lane;
         uint32_t word = i < w1 ? bm[i] : 0u;
@@ -204,28 +206,29 @@ __global__ __launch_bounds__(THREADS) void k_s2n_bitmap(ProductArgs p) {
             if (lane >= o) inc += t;
         }
         int pos = base + inc - pc;
+        if (i < w1 && (i & 7) == 0) block_rank[i >> 3] = pos;
         while (word != 0u) {
             const int b = __ffs(word) - 1;
-            if (pos < CAP) cols[pos] = i * 32 + b;
+            if (pos < nnz) cols[pos] = i * 32 + b;
             pos++;
             word &= word - 1u;
         }
         base += __shfl_sync(0xffffffffu, inc, kWarp - 1);
     }
-    __syncthreads();
     if (total != nnz && tid == 0) report(p.status, kStCapacity, row, total);
-    for (int i = tid; i < nnz; i += THREADS) {
-        p.c_col[c0 + i] = cols[i];
-        vals[i] = V(0);
-    }
+    V* out = static_cast<V*>(p.c_val) + c0;
+    for (int i = tid; i < nnz; i += THREADS) out[i] = V(0);
     __syncthreads();
     cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int ai) {
         const int32_t key = __ldg(p.b_col + qb);
-        const int pos = lower_bound_present(cols, nnz, key);
-        atomicAdd(vals + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
+        const int wi = key >> 5;
+        const int w8 = wi & ~7;
+        int rank = block_rank[wi >> 3] + __popc(bm[wi] & ((1u << (key & 31)) - 1u));
+#pragma unroll
+        for (int t = 0; t < 7; t++)
+            if (w8 + t < wi) rank += __popc(bm[w8 + t]);
+        if (rank < nnz) atomicAdd(out + rank, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
     });
-    V* out = static_cast<V*>(p.c_val) + c0;
-    for (int i = tid; i < nnz; i += THREADS) out[i] = vals[i];
 }
 
 // Global bin: a bitmap per row in flight (global scratch, B.n bits per CTA);
@@ -366,8 +369,9 @@ B200_S2N_LADDER(double)
 B200_S2N_LADDER(float)
 #undef B200_S2N_LADDER
 
-// Ladder for B.n <= kBitmapCols: rows of 3k-16k nnz use the shared-memory
-// bitmap bin instead of the hash + sort CTA bins.
+// Ladder for B.n <= kBitmapCols: every row above the 256-thread bin uses the
+// shared-memory bitmap bin (whose shared memory does not depend on the row);
+// the global bin stays last for the per-bin test knob.
 template<typename V>
 struct S2nBitmapLadder {
     static const BinLauncher entries[];
@@ -379,8 +383,8 @@ struct S2nBitmapLadder {
     const BinLauncher S2nBitmapLadder<V>::entries[] = {                                       \
         S2nLadder<V>::entries[0], S2nLadder<V>::entries[1], S2nLadder<V>::entries[2],         \
         S2nLadder<V>::entries[3], S2nLadder<V>::entries[4],                                   \
-        {BinKind::Cta, 16384, 1, 1024, BitmapLayout<V, 1024, 16384>::bytes,                   \
-         "s2n_bitmap1024", launch_bitmap<V, 1024, 16384>},                                    \
+        {BinKind::Cta, kBitmapCols, 1, 1024, BitmapLayout<V, 1024, kBitmapCols>::bytes,       \
+         "s2n_bitmap1024", launch_bitmap<V, 1024, kBitmapCols>},                              \
         {BinKind::Global, INT32_MAX, 1, 1024, 0, "s2n_global_bitmap", launch_global<V, 1024>}, \
     };                                                                                        \
     template<>                                                                                \
@@ -405,7 +409,7 @@ cudaError_t prepare_one() {
     B200_SMEM((k_s2n_cta<V, 256, 4096, 3072>), (CtaLayout<256, 4096, 3072>::bytes));
     B200_SMEM((k_s2n_cta<V, 512, 16384, 12288>), (CtaLayout<512, 16384, 12288>::bytes));
     B200_SMEM((k_s2n_cta<V, 1024, 43008, 32768>), (CtaLayout<1024, 43008, 32768>::bytes));
-    B200_SMEM((k_s2n_bitmap<V, 1024, 16384>), (BitmapLayout<V, 1024, 16384>::bytes));
+    B200_SMEM((k_s2n_bitmap<V, 1024, kBitmapCols>), (BitmapLayout<V, 1024, kBitmapCols>::bytes));
 #undef B200_SMEM
     return e;
 }
