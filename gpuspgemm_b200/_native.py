@@ -22,7 +22,7 @@ STATUS_NAMES = {
     7: "SPGEMM_ERR_INTERNAL",
 }
 
-ABI_VERSION = 2  # SPGEMM_ABI_VERSION of include/spgemm.h
+ABI_VERSION = 3  # SPGEMM_ABI_VERSION of include/spgemm.h
 
 OPT_CHECKED = 1
 OPT_MIN_SYM_BIN = 2
@@ -31,6 +31,7 @@ OPT_CLUSTER_SIZE = 4
 OPT_STREAMS = 5
 OPT_PROFILE = 6
 OPT_MIN_TRANSPOSE_BIN = 7
+OPT_ONE_PASS = 8
 
 
 class CsrView(C.Structure):
@@ -68,6 +69,7 @@ class Info(C.Structure):
         ("n_num_bins", C.c_int32),
         ("host_syncs", C.c_int32),
         ("phase_us", C.c_float * 8),
+        ("one_pass", C.c_int32),
     ]
 
 

@@ -80,6 +80,7 @@ class Handle:
             "sym_fail_rows": int(inf.sym_fail_rows),
             "host_syncs": int(inf.host_syncs),
             "phase_us": [round(float(x), 1) for x in inf.phase_us][:7],
+            "one_pass": int(inf.one_pass),
         }
 
     def profile(self) -> list[dict]:

@@ -286,6 +286,68 @@ __global__ __launch_bounds__(kBinThreads) void k_bin_scatter(
     }
 }
 
+// ---- one-pass fill: compaction of the rows into C ----------------------------
+// Row r's entries sit at [off[r], off[r] + nnz_r) of the temporary arrays (its
+// NIP-sized slot); copy them to [rpt[r], rpt[r+1]) of C.  One CTA per chunk
+// of kCompactRows rows stages the chunk's row pointers and slot offsets in
+// shared memory and walks the chunk's OUTPUT entries with consecutive threads
+// (coalesced writes; reads coalesced within rows), finding each entry's row
+// by a binary search in shared memory.
+constexpr int kCompactRows = 256;
+constexpr int kCompactThreads = 256;
+constexpr int kCompactUnroll = 4;  // independent entries per thread in flight
+
+template<typename W>
+__global__ __launch_bounds__(kCompactThreads) void k_compact_rows(
+    const int32_t* __restrict__ off, const int32_t* __restrict__ rpt, int32_t m,
+    const int32_t* __restrict__ tmp_col, const W* __restrict__ tmp_val,
+    int32_t* __restrict__ col, W* __restrict__ val) {
+    __shared__ int32_t s_rpt[kCompactRows + 1];
+    __shared__ int32_t s_off[kCompactRows];
+    const int r0 = blockIdx.x * kCompactRows;
+    const int nr = min(kCompactRows, m - r0);
+    for (int i = threadIdx.x; i <= nr; i += kCompactThreads) {
+        s_rpt[i] = rpt[r0 + i];
+        if (i < nr) s_off[i] = off[r0 + i];
+    }
+    __syncthreads();
+    const int j0 = s_rpt[0];
+    const int j1 = s_rpt[nr];
+    for (int base = j0 + threadIdx.x; base < j1; base += kCompactThreads * kCompactUnroll) {
+        int src[kCompactUnroll];
+#pragma unroll
+        for (int u = 0; u < kCompactUnroll; u++) {
+            const int j = base + u * kCompactThreads;
+            // the last row i of the chunk with s_rpt[i] <= j
+            int lo = 0;
+            int len = nr;
+            while (len > 1) {
+                const int half = len >> 1;
+                lo = s_rpt[lo + half] <= j ? lo + half : lo;
+                len -= half;
+            }
+            src[u] = s_off[lo] + (j - s_rpt[lo]);
+        }
+        int32_t c[kCompactUnroll];
+        W v[kCompactUnroll];
+#pragma unroll
+        for (int u = 0; u < kCompactUnroll; u++) {
+            if (base + u * kCompactThreads < j1) {
+                c[u] = __ldg(tmp_col + src[u]);
+                v[u] = __ldg(tmp_val + src[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kCompactUnroll; u++) {
+            const int j = base + u * kCompactThreads;
+            if (j < j1) {
+                col[j] = c[u];
+                val[j] = v[u];
+            }
+        }
+    }
+}
+
 // ---- checked mode: operand validation --------------------------------------
 __global__ void k_check_csr(const int32_t* __restrict__ rpt, const int32_t* __restrict__ col,
                             int32_t m, int32_t n, int32_t nnz, DevStatus* __restrict__ st) {
@@ -355,6 +417,22 @@ cudaError_t launch_bin_scatter(int32_t* c_rpt, int32_t m, const int32_t* hist_of
     if (g == 0) return cudaSuccess;
     k_bin_scatter<<<g, kBinThreads, 0, s>>>(c_rpt, m, hist_off, cta_off, bins, plan, lad,
                                             scan ? 1 : 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compact_rows(const int32_t* off, const int32_t* rpt, int32_t m,
+                                const int32_t* tmp_col, const void* tmp_val, int32_t* col,
+                                void* val, int value_bytes, cudaStream_t s) {
+    if (m <= 0) return cudaSuccess;
+    const int g = (m + kCompactRows - 1) / kCompactRows;
+    if (value_bytes == 8)
+        k_compact_rows<long long><<<g, kCompactThreads, 0, s>>>(
+            off, rpt, m, tmp_col, static_cast<const long long*>(tmp_val), col,
+            static_cast<long long*>(val));
+    else
+        k_compact_rows<int32_t><<<g, kCompactThreads, 0, s>>>(
+            off, rpt, m, tmp_col, static_cast<const int32_t*>(tmp_val), col,
+            static_cast<int32_t*>(val));
     return cudaGetLastError();
 }
 

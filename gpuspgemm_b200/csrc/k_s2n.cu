@@ -49,9 +49,10 @@ __global__ __launch_bounds__(THREADS) void k_s2n_team(ProductArgs p) {
     int32_t* keys = s_keys + team * T;
     const int row = p.rows[rid];
     const int c0 = p.c_rpt[row];
-    const int nnz = p.c_rpt[row + 1] - c0;
-    if (nnz > T) {
-        if (lane == 0) report(p.status, kStCapacity, row, nnz);
+    // the row's exact nnz, or in one-pass mode its NIP (an upper bound)
+    const int bound = p.c_rpt[row + 1] - c0;
+    if (bound > T) {
+        if (lane == 0) report(p.status, kStCapacity, row, bound);
         return;
     }
     for (int i = lane; i < T; i += G) keys[i] = kEmpty;
@@ -65,7 +66,13 @@ __global__ __launch_bounds__(THREADS) void k_s2n_team(ProductArgs p) {
     // sort only the row's keys: compact them to the front, then the register
     // sort leaves them in swizzled order (sort.cuh)
     const int cnt = team_compact<G>(keys, T, mask, lane);
-    if (cnt != nnz && lane == 0) report(p.status, kStCapacity, row, cnt);
+    int nnz = bound;
+    if (p.row_nnz != nullptr) {  // one-pass: the count is the row's nnz
+        nnz = cnt;
+        if (lane == 0) p.row_nnz[row] = cnt;
+    } else if (cnt != nnz && lane == 0) {
+        report(p.status, kStCapacity, row, cnt);
+    }
     team_sort_swz<G, T / G>(keys, cnt, mask, lane);
     V* out = static_cast<V*>(p.c_val) + c0;
     for (int i = lane; i < nnz; i += G) {
@@ -97,9 +104,10 @@ __global__ __launch_bounds__(THREADS) void k_s2n_cta(ProductArgs p) {
     auto& sc = *reinterpret_cast<CtaScratch<THREADS>*>(smem_raw + L::keys_bytes);
     const int row = p.rows[blockIdx.x];
     const int c0 = p.c_rpt[row];
-    const int nnz = p.c_rpt[row + 1] - c0;
-    if (nnz > CAP) {
-        if (threadIdx.x == 0) report(p.status, kStCapacity, row, nnz);
+    // the row's exact nnz, or in one-pass mode its NIP (an upper bound)
+    const int bound = p.c_rpt[row + 1] - c0;
+    if (bound > CAP) {
+        if (threadIdx.x == 0) report(p.status, kStCapacity, row, bound);
         return;
     }
     for (int i = threadIdx.x; i < T; i += THREADS) keys[i] = kEmpty;
@@ -110,7 +118,13 @@ __global__ __launch_bounds__(THREADS) void k_s2n_cta(ProductArgs p) {
         table_insert(keys, T, __ldg(p.b_col + qb), p.status, row);
     });
     const int cnt = cta_compact<THREADS>(keys, T, sc.warp_tot);
-    if (cnt != nnz && threadIdx.x == 0) report(p.status, kStCapacity, row, cnt);
+    int nnz = bound;
+    if (p.row_nnz != nullptr) {  // one-pass: the count is the row's nnz
+        nnz = cnt <= CAP ? cnt : CAP;
+        if (threadIdx.x == 0) p.row_nnz[row] = nnz;
+    } else if (cnt != nnz && threadIdx.x == 0) {
+        report(p.status, kStCapacity, row, cnt);
+    }
     // register sort of the row's keys; they come back in swizzled order
     static_assert(L::K >= THREADS * 16, "the register sort needs THREADS * 16 key slots");
     // (cnt > CAP only for an invalid operand, reported above; the clamp keeps
@@ -162,10 +176,11 @@ __global__ __launch_bounds__(THREADS) void k_s2n_bitmap(ProductArgs p) {
     const int w = tid >> 5;
     const int row = p.rows[blockIdx.x];
     const int c0 = p.c_rpt[row];
-    const int nnz = p.c_rpt[row + 1] - c0;
+    // the row's exact nnz, or in one-pass mode its NIP (an upper bound)
+    const int bound = p.c_rpt[row + 1] - c0;
     const int words = (p.n_cols + 31) >> 5;
-    if (nnz > CAP || words > kBitmapWords) {
-        if (tid == 0) report(p.status, kStCapacity, row, nnz);
+    if (bound > CAP || words > kBitmapWords) {
+        if (tid == 0) report(p.status, kStCapacity, row, bound);
         return;
     }
     for (int i = tid; i < words; i += THREADS) bm[i] = 0u;
@@ -209,13 +224,19 @@ __global__ __launch_bounds__(THREADS) void k_s2n_bitmap(ProductArgs p) {
         if (i < w1 && (i & 7) == 0) block_rank[i >> 3] = pos;
         while (word != 0u) {
             const int b = __ffs(word) - 1;
-            if (pos < nnz) cols[pos] = i * 32 + b;
+            if (pos < bound) cols[pos] = i * 32 + b;
             pos++;
             word &= word - 1u;
         }
         base += __shfl_sync(0xffffffffu, inc, kWarp - 1);
     }
-    if (total != nnz && tid == 0) report(p.status, kStCapacity, row, total);
+    int nnz = bound;
+    if (p.row_nnz != nullptr) {  // one-pass: the count is the row's nnz
+        nnz = total <= bound ? total : bound;
+        if (tid == 0) p.row_nnz[row] = nnz;
+    } else if (total != nnz && tid == 0) {
+        report(p.status, kStCapacity, row, total);
+    }
     V* out = static_cast<V*>(p.c_val) + c0;
     for (int i = tid; i < nnz; i += THREADS) out[i] = V(0);
     __syncthreads();
@@ -244,7 +265,8 @@ __global__ __launch_bounds__(THREADS) void k_s2n_global(ProductArgs p) {
     for (int rid = blockIdx.x; rid < p.nrows; rid += gridDim.x) {
         const int row = p.rows[rid];
         const int c0 = p.c_rpt[row];
-        const int nnz = p.c_rpt[row + 1] - c0;
+        // the row's exact nnz, or in one-pass mode its NIP (an upper bound)
+        const int bound = p.c_rpt[row + 1] - c0;
         const int a0 = p.a_rpt[row];
         const int a1 = p.a_rpt[row + 1];
         const int2 win = cta_col_window<THREADS>(p.a_col, p.b_rpt, p.b_col, a0, a1, p.n_cols, sc);
@@ -284,14 +306,20 @@ __global__ __launch_bounds__(THREADS) void k_s2n_global(ProductArgs p) {
             int pos = base + inc - cnt;
             while (w != 0u) {
                 const int b = __ffs(w) - 1;
-                if (pos < nnz) cols[pos] = (w0 + wi) * 32 + b;
+                if (pos < bound) cols[pos] = (w0 + wi) * 32 + b;
                 pos++;
                 w &= w - 1u;
             }
             base += sc.warp_tot[THREADS / kWarp - 1];
             __syncthreads();
         }
-        if (base != nnz && threadIdx.x == 0) report(p.status, kStCapacity, row, base);
+        int nnz = bound;
+        if (p.row_nnz != nullptr) {  // one-pass: the count is the row's nnz
+            nnz = base <= bound ? base : bound;
+            if (threadIdx.x == 0) p.row_nnz[row] = nnz;
+        } else if (base != nnz && threadIdx.x == 0) {
+            report(p.status, kStCapacity, row, base);
+        }
         V* out = static_cast<V*>(p.c_val) + c0;
         for (int i = threadIdx.x; i < nnz; i += THREADS) out[i] = V(0);
         __syncthreads();

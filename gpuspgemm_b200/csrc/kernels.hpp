@@ -57,6 +57,10 @@ struct ProductArgs {
     int32_t* fail_count;
     // transpose: per entry of T, (row of A << 32 | position in A)
     uint64_t* keys;
+    // one-pass fill: c_rpt gives each row a slot of its NIP entries (an upper
+    // bound); the kernel writes the row's exact nnz here (nullptr: c_rpt is
+    // C's exact row pointer)
+    int32_t* row_nnz;
 };
 
 enum class BinKind : int { Team = 0, Cta = 1, Cluster = 2, Global = 3 };
@@ -71,6 +75,12 @@ struct BinLauncher {
     cudaError_t (*launch)(const ProductArgs&, cudaStream_t);
 };
 
+// One-pass fill (no count phase) when its temporaries, NIP entries of column
+// and value, fit this many bytes and the product has at least kOnePassMinNip
+// intermediate products (below that its extra host synchronisation and
+// launches cost more than the count phase it saves).
+constexpr uint64_t kOnePassMaxBytes = uint64_t(4) << 30;
+constexpr int64_t kOnePassMinNip = int64_t(1) << 21;
 // Symbolic count ladder (key = NIP of the row).
 int sym1_ladder(const BinLauncher** out);
 // Fused fill + sort + numeric ladder (key = nnz of the row), per value type.
@@ -107,6 +117,11 @@ cudaError_t launch_bin_offsets(int32_t* hist, int32_t nctas, int64_t* cta_sum, P
 cudaError_t launch_bin_scatter(int32_t* c_rpt, int32_t m, const int32_t* hist_off,
                                const int64_t* cta_off, int32_t* bins, const Plan* plan,
                                const Ladder& lad, bool scan, cudaStream_t s);
+// One-pass fill: copy each row's entries from its slot [off[r], ...) of the
+// temporary arrays to [rpt[r], rpt[r+1]) of C (values of value_bytes 4 or 8).
+cudaError_t launch_compact_rows(const int32_t* off, const int32_t* rpt, int32_t m,
+                                const int32_t* tmp_col, const void* tmp_val, int32_t* col,
+                                void* val, int value_bytes, cudaStream_t s);
 // Operand validation (checked mode).
 cudaError_t launch_check_csr(const int32_t* rpt, const int32_t* col, int32_t m, int32_t n,
                              int32_t nnz, DevStatus* st, cudaStream_t s);

@@ -107,6 +107,7 @@ struct spgemm_handle_s {
     int cluster = 4;
     int profile = 0;
     int min_tr_bin = -1;
+    int one_pass = 0;  // 0 chosen by temporary size, 1 always, 2 never (two-pass)
     // C's arrays come from the device's shared stream-ordered pool (see
     // device_pool); it keeps freed memory mapped so repeated products do not
     // re-map hundreds of MB per call.  cudaFree / cudaFreeAsync release them.
@@ -493,6 +494,145 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     pa.fail_rows = s.fail_rows;
     pa.fail_count = s.fail_count;
     pa.words = (static_cast<int64_t>(n) + 31) / 32;
+
+    // ---- one-pass fill: no count phase ------------------------------------
+    // Rows are binned by NIP (an upper bound of their nnz) on the fill ladder
+    // and filled into NIP-sized slots of temporary arrays; each fill kernel
+    // records its row's exact nnz in C.rpt, which a scan turns into the row
+    // pointer, and the rows are then compacted into C.  That replaces the count
+    // kernels, the scan binning and their second pass over every product with
+    // one copy of C, at the price of temporaries of NIP entries.  Plans keep
+    // the two-pass path (their graph replays the fill alone).
+    const int64_t nip_total = p1.total_key;
+    const bool one_pass =
+        cr == nullptr && h->one_pass != 2 && nip_total <= INT32_MAX &&
+        (h->one_pass == 1 ||
+         (nip_total >= kOnePassMinNip &&
+          static_cast<uint64_t>(nip_total) * (4 + sizeof(V)) <= kOnePassMaxBytes));
+    h->info.one_pass = one_pass ? 1 : 0;
+    if (one_pass) {
+        int32_t* off = nullptr;
+        int32_t* tmp_col = nullptr;
+        void* tmp_val = nullptr;
+        auto release = [&]() {
+            if (off) cudaFreeAsync(off, stream);
+            if (tmp_col) cudaFreeAsync(tmp_col, stream);
+            if (tmp_val) cudaFreeAsync(tmp_val, stream);
+        };
+#define B200_ONE(expr)                                                   \
+    do {                                                                 \
+        spgemm_status st_ = (expr);                                      \
+        if (st_ != SPGEMM_OK) {                                          \
+            release();                                                   \
+            return bail(st_);                                            \
+        }                                                                \
+    } while (0)
+#define B200_ONE_CUDA(expr, what)                                        \
+    do {                                                                 \
+        cudaError_t e_ = (expr);                                         \
+        if (e_ != cudaSuccess) {                                         \
+            release();                                                   \
+            return bail(cuda_fail(e_, what));                            \
+        }                                                                \
+    } while (0)
+        // NIP slots: the scan of the NIP per row (c_rpt holds it) into off
+        B200_ONE_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&off),
+                                              sizeof(int32_t) * (size_t(m) + 1), h->pool, stream),
+                      "allocate NIP slots");
+        B200_ONE_CUDA(cudaMemcpyAsync(off, c_rpt, sizeof(int32_t) * size_t(m),
+                                      cudaMemcpyDeviceToDevice, stream),
+                      "copy NIP per row");
+        const Ladder ladf = make_ladder(fil, nfil, h->min_num_bin);
+        B200_ONE(timed(h, "nip_fill_hist", 2, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_nnz_hist(off, m, s.hist2, s.cta_sum, s.plan2, ladf, ss);
+        }));
+        B200_ONE(timed(h, "nip_fill_offsets", 2, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_bin_offsets(s.hist2, nctas, s.cta_sum, s.plan2, ladf, ss);
+        }));
+        B200_ONE(timed(h, "nip_fill_scatter", 2, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_bin_scatter(off, m, s.hist2, s.cta_sum, s.bins2, s.plan2, ladf, true,
+                                      ss);
+        }));
+        // C.rpt receives each row's exact nnz (rows without products stay 0)
+        B200_ONE_CUDA(cudaMemsetAsync(c_rpt, 0, sizeof(int32_t) * (size_t(m) + 1), stream),
+                      "memset row counts");
+        B200_ONE_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&tmp_col),
+                                              sizeof(int32_t) * size_t(nip_total) + 16, h->pool,
+                                              stream),
+                      "allocate the one-pass columns");
+        B200_ONE_CUDA(cudaMallocFromPoolAsync(&tmp_val, sizeof(V) * size_t(nip_total), h->pool,
+                                              stream),
+                      "allocate the one-pass values");
+        mark(2);
+        B200_ONE(sync_mirror(h, stream, s.plan2, s));
+        mark(3);
+        B200_ONE(status_to_error(h->mirror->status));
+        const Plan pf = h->mirror->plan;
+        for (int b = 0; b < nfil && b < 16; b++) h->info.num_bin_rows[b] = pf.bin_size[b];
+        pa.c_rpt = off;
+        pa.c_col = tmp_col;
+        pa.c_val = tmp_val;
+        pa.row_nnz = c_rpt;
+        if (pf.bin_size[nfil - 1] > 0) {
+            int32_t nmaps = 0;
+            B200_ONE(ensure_bitmaps(h, pa.words, pf.bin_size[nfil - 1], &nmaps, stream));
+            pa.bitmaps = h->bitmaps;
+            pa.nmaps = nmaps;
+        }
+        mark(4);
+        B200_ONE(launch_bins(h, fil, nfil, 3, pf, s.bins2, pa, stream));
+        // row pointer from the counts: a one-bin pass with the scan, into the
+        // count binning's plan (reset: its max and overflow only ever grow)
+        B200_ONE_CUDA(cudaMemsetAsync(s.plan1, 0, sizeof(Plan), stream), "reset a plan");
+        Ladder one = {};
+        one.nb = 1;
+        one.limit[0] = INT32_MAX;
+        B200_ONE(timed(h, "count_scan_hist", 2, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_nnz_hist(c_rpt, m, s.hist1, s.cta_sum, s.plan1, one, ss);
+        }));
+        B200_ONE(timed(h, "count_scan_offsets", 2, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_bin_offsets(s.hist1, nctas, s.cta_sum, s.plan1, one, ss);
+        }));
+        B200_ONE(timed(h, "count_scan_scatter", 2, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_bin_scatter(c_rpt, m, s.hist1, s.cta_sum, s.bins1, s.plan1, one, true,
+                                      ss);
+        }));
+        mark(5);
+        B200_ONE(sync_mirror(h, stream, s.plan1, s));
+        B200_ONE(status_to_error(h->mirror->status));
+        const Plan pc = h->mirror->plan;
+        if (pc.overflow || pc.total_key > nip_total)
+            return release(), bail(fail(SPGEMM_ERR_INTERNAL, "one-pass row counts out of range"));
+        const int32_t nnz = static_cast<int32_t>(pc.total_key);
+        h->info.nnz = nnz;
+        h->info.max_row_nnz = pc.max_key;
+        C->nnz = nnz;
+        if (nnz > 0) {
+            B200_ONE_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&C->col),
+                                                  sizeof(int32_t) * size_t(nnz) + 16, h->pool,
+                                                  stream),
+                          "allocate C.col");
+            B200_ONE_CUDA(cudaMallocFromPoolAsync(&C->val, sizeof(V) * size_t(nnz), h->pool,
+                                                  stream),
+                          "allocate C.val");
+            B200_ONE(timed(h, "compact_rows", 3, -1, m, stream, [&](cudaStream_t ss) {
+                return launch_compact_rows(off, c_rpt, m, tmp_col, tmp_val, C->col, C->val,
+                                           static_cast<int>(sizeof(V)), ss);
+            }));
+        }
+        release();
+        off = nullptr;
+        tmp_col = nullptr;
+        tmp_val = nullptr;
+        if (cudaError_t e = cudaStreamSynchronize(stream); e != cudaSuccess)
+            return bail(cuda_fail(e, "final synchronize"));
+        mark(6);
+        h->info.host_syncs++;
+        resolve_profile(h);
+#undef B200_ONE_CUDA
+#undef B200_ONE
+        return SPGEMM_OK;
+    }
 
     // ---- sym1: exact nnz per row --------------------------------------------
     const int glob1 = nsym - 1;  // global bin (cluster spills, or the test knob)
@@ -1769,6 +1909,11 @@ spgemm_status spgemm_set_option(spgemm_handle_t h, spgemm_option opt, int64_t va
             return SPGEMM_OK;
         case SPGEMM_OPT_PROFILE: h->profile = value != 0; return SPGEMM_OK;
         case SPGEMM_OPT_MIN_TRANSPOSE_BIN: h->min_tr_bin = static_cast<int>(value); return SPGEMM_OK;
+        case SPGEMM_OPT_ONE_PASS:
+            if (value < 0 || value > 2)
+                return fail(SPGEMM_ERR_INVALID_ARG, "one-pass must be 0, 1 or 2");
+            h->one_pass = static_cast<int>(value);
+            return SPGEMM_OK;
     }
     return fail(SPGEMM_ERR_INVALID_ARG, "unknown option");
 }
@@ -1783,6 +1928,7 @@ spgemm_status spgemm_get_option(spgemm_handle_t h, spgemm_option opt, int64_t* v
         case SPGEMM_OPT_STREAMS: *value = h->nside; return SPGEMM_OK;
         case SPGEMM_OPT_PROFILE: *value = h->profile; return SPGEMM_OK;
         case SPGEMM_OPT_MIN_TRANSPOSE_BIN: *value = h->min_tr_bin; return SPGEMM_OK;
+        case SPGEMM_OPT_ONE_PASS: *value = h->one_pass; return SPGEMM_OK;
     }
     return fail(SPGEMM_ERR_INVALID_ARG, "unknown option");
 }

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define SPGEMM_ABI_VERSION 2
+#define SPGEMM_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define SPGEMM_API __attribute__((visibility("default")))
@@ -99,6 +99,7 @@ typedef struct spgemm_info {
      * host sync 1 done, count kernels queued, host sync 2 done, C allocated,
      * fill kernels queued, final sync done (unused entries 0) */
     float phase_us[8];
+    int32_t one_pass;        /* 1: C's row sizes came from the one-pass fill */
 } spgemm_info;
 
 /* ---- lifecycle ------------------------------------------------------------ */
@@ -180,7 +181,15 @@ typedef enum spgemm_option {
     SPGEMM_OPT_PROFILE = 6,
     /* Test knob: every non-empty row of a transpose goes to at least this bin
      * of its row-sort ladder (-1 = off). */
-    SPGEMM_OPT_MIN_TRANSPOSE_BIN = 7
+    SPGEMM_OPT_MIN_TRANSPOSE_BIN = 7,
+    /* How the row sizes of C are found.  0 (default): one pass when the
+     * product has at least 2^21 intermediate products (NIP) and its
+     * temporaries -- NIP entries of column and value -- fit 4 GiB, else two;
+     * 1: always one pass; 2: always two passes.  Two passes: the hash count
+     * kernels give each row's exact nnz, the fill writes C in place.  One
+     * pass: rows are filled into NIP-sized slots while their nnz is counted,
+     * then compacted into C -- no count kernels, one more copy of C. */
+    SPGEMM_OPT_ONE_PASS = 8
 } spgemm_option;
 
 SPGEMM_API spgemm_status spgemm_set_option(spgemm_handle_t handle, spgemm_option option, int64_t value);

@@ -96,10 +96,13 @@ def test_forced_sym_bin(handle, oracle_mod, b):
         pytest.skip("no such bin")
     A = G.power_law(3000, 2.0, 300, seed=41)
     handle.set_option(N.OPT_MIN_SYM_BIN, b)
+    handle.set_option(N.OPT_ONE_PASS, 2)  # the count kernels run in two-pass mode only
     try:
         C = gpu_product(A, A, handle, np.float64)
+        assert handle.info()["one_pass"] == 0
     finally:
         handle.set_option(N.OPT_MIN_SYM_BIN, -1)
+        handle.set_option(N.OPT_ONE_PASS, 0)
     check(oracle_mod, A, A, C, np.float64, f"forced_sym_bin{b}", positive=True)
 
 
@@ -113,7 +116,10 @@ def _wide_pair():
 @pytest.mark.parametrize("b", range(9))
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 @pytest.mark.parametrize("width", ["narrow", "wide"])
-def test_forced_num_bin(handle, oracle_mod, b, dtype, width):
+@pytest.mark.parametrize("passes", [1, 2])
+def test_forced_num_bin(handle, oracle_mod, b, dtype, width, passes):
+    """Every row routed to at least fill bin b, with C's row sizes from the
+    one-pass fill (bins keyed by NIP) or from the count kernels (by nnz)."""
     from gpuspgemm_b200 import _native as N
     which = 2 if width == "narrow" else 1
     if b >= len(handle.ladder(which, 8)):
@@ -124,11 +130,14 @@ def test_forced_num_bin(handle, oracle_mod, b, dtype, width):
     else:
         A, B = _wide_pair()
     handle.set_option(N.OPT_MIN_NUM_BIN, b)
+    handle.set_option(N.OPT_ONE_PASS, passes)
     try:
         C = gpu_product(A, B, handle, dtype)
+        assert handle.info()["one_pass"] == (1 if passes == 1 else 0)
     finally:
         handle.set_option(N.OPT_MIN_NUM_BIN, -1)
-    check(oracle_mod, A, B, C, dtype, f"forced_num_bin{b}_{width}", positive=True)
+        handle.set_option(N.OPT_ONE_PASS, 0)
+    check(oracle_mod, A, B, C, dtype, f"forced_num_bin{b}_{width}_pass{passes}", positive=True)
 
 
 @pytest.mark.parametrize("shuffle", [False, True])
@@ -150,11 +159,18 @@ def test_global_bins_block_diagonal(handle, oracle_mod, shuffle):
             B.val[s:e] = B.val[s:e][p]
     handle.set_option(N.OPT_MIN_SYM_BIN, _ladder_len(handle, 0) - 1)
     handle.set_option(N.OPT_MIN_NUM_BIN, _ladder_len(handle, 2) - 1)
+    handle.set_option(N.OPT_ONE_PASS, 2)
     try:
         C = gpu_product(A, B, handle, np.float64)
+        # the same rows in the one-pass fill's global bin
+        handle.set_option(N.OPT_ONE_PASS, 1)
+        C1 = gpu_product(A, B, handle, np.float64)
     finally:
         handle.set_option(N.OPT_MIN_SYM_BIN, -1)
         handle.set_option(N.OPT_MIN_NUM_BIN, -1)
+        handle.set_option(N.OPT_ONE_PASS, 0)
+    check(oracle_mod, A, A, C1, np.float64, f"global_blockdiag_onepass{int(shuffle)}",
+          positive=True)
     check(oracle_mod, A, A, C, np.float64, f"global_blockdiag_shuffle{int(shuffle)}",
           positive=True)
 
@@ -192,14 +208,44 @@ def test_long_rows_wide_cta_bins(handle, oracle_mod, dtype):
     check(oracle_mod, A, B, C, dtype, "long_rows_wide", positive=True)
 
 
-def test_high_compression_stencil(handle, oracle_mod):
+@pytest.mark.parametrize("passes", [1, 2])
+def test_high_compression_stencil(handle, oracle_mod, passes):
     """A 27-point stencil squared: ~5.9 products per entry of C, all
-    accumulated with global reductions into the row's slice of C.val."""
+    accumulated with global reductions into the row's slice of C.val; in
+    one-pass mode each row's slot holds its NIP entries, ~6x its nnz."""
+    from gpuspgemm_b200 import _native as N
     S = G.stencil27(20)
-    C = gpu_product(S, S, handle, np.float64)
-    info = handle.info()
-    assert info["nip"] > 5 * info["nnz"]
-    check(oracle_mod, S, S, C, np.float64, "stencil20_squared")
+    handle.set_option(N.OPT_ONE_PASS, passes)
+    try:
+        C = gpu_product(S, S, handle, np.float64)
+        info = handle.info()
+    finally:
+        handle.set_option(N.OPT_ONE_PASS, 0)
+    assert info["nip"] > 5 * info["nnz"] and info["one_pass"] == (passes == 1)
+    check(oracle_mod, S, S, C, np.float64, f"stencil20_squared_pass{passes}")
+
+
+def test_one_pass_chosen_and_equal_to_two_pass(handle, oracle_mod):
+    """By default a product whose temporaries fit runs one pass; its C equals
+    the two-pass C in structure, and both match the oracle."""
+    from gpuspgemm_b200 import _native as N
+    A = G.power_law(200000, 2.0, 3000, seed=25)  # NIP above the one-pass minimum
+    C1 = gpu_product(A, A, handle, np.float64)
+    info1 = handle.info()
+    assert info1["one_pass"] == 1 and info1["nip"] >= 1 << 21
+    S = G.uniform_rows(4096, 8)  # a small product keeps two passes
+    gpu_product(S, S, handle, np.float64)
+    assert handle.info()["one_pass"] == 0
+    handle.set_option(N.OPT_ONE_PASS, 2)
+    try:
+        C2 = gpu_product(A, A, handle, np.float64)
+        info2 = handle.info()
+    finally:
+        handle.set_option(N.OPT_ONE_PASS, 0)
+    assert info2["one_pass"] == 0 and info2["host_syncs"] == 3 and info1["host_syncs"] == 4
+    assert np.array_equal(C1.rpt, C2.rpt) and np.array_equal(C1.col, C2.col)
+    assert info1["nnz"] == info2["nnz"] and info1["max_row_nnz"] == info2["max_row_nnz"]
+    check(oracle_mod, A, A, C1, np.float64, "one_pass_default", positive=True)
 
 
 def test_heavy_row_spills_to_global(handle, oracle_mod):
@@ -211,8 +257,13 @@ def test_heavy_row_spills_to_global(handle, oracle_mod):
     A = HostCSR(3, 1000, np.array([0, 1000, 1000, 1003], np.int32),
                 np.concatenate([a_col, np.array([1, 5, 9], np.int32)]),
                 rng.uniform(0.1, 1.0, 1003))
-    C = gpu_product(A, B, handle, np.float64)
-    info = handle.info()
+    from gpuspgemm_b200 import _native as N
+    handle.set_option(N.OPT_ONE_PASS, 2)  # the cluster table and its spill
+    try:
+        C = gpu_product(A, B, handle, np.float64)
+        info = handle.info()
+    finally:
+        handle.set_option(N.OPT_ONE_PASS, 0)
     check(oracle_mod, A, B, C, np.float64, "heavy_row_spill", positive=False)
     assert info["max_row_nnz"] > 150_000
 
