@@ -22,7 +22,7 @@ STATUS_NAMES = {
     7: "SPGEMM_ERR_INTERNAL",
 }
 
-ABI_VERSION = 3  # SPGEMM_ABI_VERSION of include/spgemm.h
+ABI_VERSION = 4  # SPGEMM_ABI_VERSION of include/spgemm.h
 
 OPT_CHECKED = 1
 OPT_MIN_SYM_BIN = 2
@@ -32,6 +32,7 @@ OPT_STREAMS = 5
 OPT_PROFILE = 6
 OPT_MIN_TRANSPOSE_BIN = 7
 OPT_ONE_PASS = 8
+OPT_ESC = 9
 
 
 class CsrView(C.Structure):
@@ -70,6 +71,7 @@ class Info(C.Structure):
         ("host_syncs", C.c_int32),
         ("phase_us", C.c_float * 8),
         ("one_pass", C.c_int32),
+        ("esc_mask", C.c_int32),
     ]
 
 

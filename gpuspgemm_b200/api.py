@@ -81,6 +81,7 @@ class Handle:
             "host_syncs": int(inf.host_syncs),
             "phase_us": [round(float(x), 1) for x in inf.phase_us][:7],
             "one_pass": int(inf.one_pass),
+            "esc_mask": int(inf.esc_mask),
         }
 
     def profile(self) -> list[dict]:

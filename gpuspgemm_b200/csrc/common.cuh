@@ -99,15 +99,18 @@ __device__ __forceinline__ void team_sync(unsigned mask) {
 }
 
 // Walk the intermediate products of the A-row segment [a0, a1) with a team of
-// G lanes.  For every product, calls f(q_b, a_index) where q_b is the position
-// of the B entry in B.col / B.val and a_index the position of the A entry.
-// All lanes of the team must call this together (the shuffles are team-wide).
+// G lanes.  For every product, calls f(q_b, a_index, q) where q_b is the
+// position of the B entry in B.col / B.val, a_index the position of the A
+// entry and q the product's place in the row's flattened sequence (products
+// of A entry a0 first, each B row in order).  All lanes of the team must call
+// this together (the shuffles are team-wide).
 template<int G, typename F>
-__device__ __forceinline__ void team_for_products(const int32_t* __restrict__ a_col,
-                                                  const int32_t* __restrict__ b_rpt, int a0,
-                                                  int a1, F&& f) {
+__device__ __forceinline__ void team_for_products_at(const int32_t* __restrict__ a_col,
+                                                     const int32_t* __restrict__ b_rpt, int a0,
+                                                     int a1, F&& f) {
     const unsigned mask = team_mask<G>();
     const int lane = team_lane<G>();
+    int off = 0;
     for (int base = a0; base < a1; base += G) {
         const int e = base + lane;
         int bs = 0;
@@ -132,9 +135,18 @@ __device__ __forceinline__ void team_for_products(const int32_t* __restrict__ a_
             }
             const int sbs = __shfl_sync(mask, bs, s, G);
             const int sexc = __shfl_sync(mask, exc, s, G);
-            if (q < total) f(sbs + q - sexc, base + s);
+            if (q < total) f(sbs + q - sexc, base + s, off + q);
         }
+        off += total;
     }
+}
+
+// The same walk for callers that need no product position: f(q_b, a_index).
+template<int G, typename F>
+__device__ __forceinline__ void team_for_products(const int32_t* __restrict__ a_col,
+                                                  const int32_t* __restrict__ b_rpt, int a0,
+                                                  int a1, F&& f) {
+    team_for_products_at<G>(a_col, b_rpt, a0, a1, [&](int qb, int ai, int) { f(qb, ai); });
 }
 
 // lower_bound over a sorted int array of length n (n >= 1); the key is known to

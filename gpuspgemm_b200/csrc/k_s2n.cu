@@ -87,6 +87,142 @@ __global__ __launch_bounds__(THREADS) void k_s2n_team(ProductArgs p) {
     });
 }
 
+// Expand-sort-compress fill of rows with at most NMAX products, for the
+// one-pass mode (rows binned by NIP, each filling a NIP-sized slot).  One walk
+// over the row's products stages every product in shared memory: its value
+// c = a_ik * b_kj, and the key (column << SHIFT | q), q the product's place in
+// the row.  The team's register sort orders the keys by column and, within a
+// column, by q.  The first product of each column run then sums the run's
+// values in that order and writes the column and the sum to the next slot.
+// That needs no hash table, no second walk of the products, no binary search
+// and no atomics, and sums each entry of C in the oracle's (Gustavson) order.
+// The keys need B.n <= 2^(31 - SHIFT); the ladder that holds these kernels is
+// used only for B.n <= kBitmapCols = 2^20 (SHIFT <= 10).
+constexpr int ilog2(int x) { return x <= 1 ? 0 : 1 + ilog2(x >> 1); }
+
+template<typename V, int G, int THREADS, int NMAX>
+struct EscLayout {
+    static constexpr int T = next_pow2(NMAX);  // sort capacity of a team
+    static constexpr int SHIFT = ilog2(T);
+    static constexpr size_t vals_bytes = sizeof(V) * NMAX * (THREADS / G);
+    static constexpr size_t bytes = vals_bytes + sizeof(int32_t) * T * (THREADS / G);
+    static_assert(SHIFT <= 10, "column keys of an ESC bin need 31 - SHIFT >= 21 bits");
+};
+
+template<typename V, int G, int THREADS, int NMAX>
+__global__ __launch_bounds__(THREADS) void k_esc_team(ProductArgs p) {
+    using L = EscLayout<V, G, THREADS, NMAX>;
+    constexpr int R = THREADS / G;
+    constexpr int T = L::T;
+    constexpr int SHIFT = L::SHIFT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int team = threadIdx.x / G;
+    const int lane = team_lane<G>();
+    const unsigned mask = team_mask<G>();
+    const int rid = blockIdx.x * R + team;
+    if (rid >= p.nrows) return;
+    V* vals = reinterpret_cast<V*>(smem_raw) + team * NMAX;
+    int32_t* keys = reinterpret_cast<int32_t*>(smem_raw + L::vals_bytes) + team * T;
+    const int row = p.rows[rid];
+    const int c0 = p.c_rpt[row];
+    const int nip = p.c_rpt[row + 1] - c0;  // the row's NIP-sized slot
+    if (nip > NMAX || p.row_nnz == nullptr) {
+        if (lane == 0) report(p.status, kStCapacity, row, nip);
+        return;
+    }
+    team_for_products_at<G>(p.a_col, p.b_rpt, p.a_rpt[row], p.a_rpt[row + 1],
+                            [&](int qb, int ai, int q) {
+                                if (q < NMAX) {
+                                    keys[q] = (__ldg(p.b_col + qb) << SHIFT) | q;
+                                    vals[q] = ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb);
+                                }
+                            });
+    team_sync<G>(mask);
+    team_sort_swz<G, T / G>(keys, nip, mask, lane);
+    int32_t* out_col = p.c_col + c0;
+    V* out_val = static_cast<V*>(p.c_val) + c0;
+    const unsigned below = (1u << (threadIdx.x & 31u)) - 1u;
+    int written = 0;
+    int carry = -1;  // column of the element before the chunk
+    for (int i0 = 0; i0 < nip; i0 += G) {
+        const int i = i0 + lane;
+        const int32_t key = i < nip ? keys[swz(i)] : kEmpty;
+        const int col = key >> SHIFT;
+        int prev = __shfl_up_sync(mask, col, 1, G);
+        if (lane == 0) prev = carry;
+        const bool head = i < nip && col != prev;
+        const unsigned bits = __ballot_sync(mask, head) & mask;
+        if (head) {
+            V sum = vals[key & (T - 1)];
+            for (int k = i + 1; k < nip; k++) {
+                const int32_t next = keys[swz(k)];
+                if ((next >> SHIFT) != col) break;
+                sum += vals[next & (T - 1)];
+            }
+            const int r = written + __popc(bits & below);
+            out_col[r] = col;
+            out_val[r] = sum;
+        }
+        written += __popc(bits);
+        carry = __shfl_sync(mask, col, G - 1, G);
+    }
+    if (lane == 0) p.row_nnz[row] = written;
+}
+
+// Compression of the team bins, sampled: `samples` rows spread evenly over
+// A are counted exactly (one warp per row, a 1024-slot shared hash set) when
+// their NIP is at most the last team bin's limit, and their NIP and nnz are
+// summed per team bin (binned by NIP with the ladder's limits).  It needs A
+// and B only, so it runs beside the fill binning; the host reads the sums
+// with the binning plan and lets a team bin expand-sort-compress only when
+// its rows repeat few columns: ESC sorts every product, the hash bins only
+// the distinct columns.
+constexpr int kSampleWarps = 8;
+constexpr int kSampleSlots = 1024;
+
+__global__ __launch_bounds__(kSampleWarps * kWarp) void k_esc_sample(ProductArgs p, int32_t m,
+                                                                      int32_t samples,
+                                                                      EscLimits lim,
+                                                                      EscSample* out) {
+    __shared__ int32_t s_tab[kSampleWarps][kSampleSlots];
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    const int w = blockIdx.x * kSampleWarps + wid;
+    if (w >= samples) return;
+    const int row = static_cast<int>(static_cast<int64_t>(w) * m / samples);
+    const int a0 = p.a_rpt[row];
+    const int a1 = p.a_rpt[row + 1];
+    const int cap = lim.limit[kEscBins - 1];
+    if (a1 - a0 > cap) return;  // more products than the team bins take
+    int nip = 0;
+    for (int e = a0 + lane; e < a1; e += kWarp) {
+        const int c = __ldg(p.a_col + e);
+        nip += __ldg(p.b_rpt + c + 1) - __ldg(p.b_rpt + c);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nip += __shfl_xor_sync(0xffffffffu, nip, o);
+    if (nip == 0 || nip > cap || nip > 3 * kSampleSlots / 4) return;
+    int b = 0;
+    while (nip > lim.limit[b]) b++;
+    int32_t* tab = s_tab[wid];
+    for (int i = lane; i < kSampleSlots; i += kWarp) tab[i] = kEmpty;
+    __syncwarp();
+    team_for_products<kWarp>(p.a_col, p.b_rpt, a0, a1, [&](int qb, int) {
+        table_insert(tab, kSampleSlots, __ldg(p.b_col + qb), p.status, row);
+    });
+    __syncwarp();
+    int cnt = 0;
+    for (int i = lane; i < kSampleSlots; i += kWarp) cnt += tab[i] != kEmpty;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(&out->nip[b]),
+                  static_cast<unsigned long long>(nip));
+        atomicAdd(reinterpret_cast<unsigned long long*>(&out->nnz[b]),
+                  static_cast<unsigned long long>(cnt));
+    }
+}
+
 template<int THREADS, int T, int CAP>
 struct CtaLayout {
     static constexpr int P = next_pow2(CAP);
@@ -344,6 +480,15 @@ cudaError_t launch_team(const ProductArgs& p, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template<typename V, int G, int THREADS, int NMAX>
+cudaError_t launch_esc(const ProductArgs& p, cudaStream_t s) {
+    constexpr int R = THREADS / G;
+    const int grid = (p.nrows + R - 1) / R;
+    k_esc_team<V, G, THREADS, NMAX>
+        <<<grid, THREADS, EscLayout<V, G, THREADS, NMAX>::bytes, s>>>(p);
+    return cudaGetLastError();
+}
+
 template<typename V, int THREADS, int T, int CAP>
 cudaError_t launch_cta(const ProductArgs& p, cudaStream_t s) {
     k_s2n_cta<V, THREADS, T, CAP>
@@ -423,6 +568,36 @@ B200_S2N_BITMAP_LADDER(double)
 B200_S2N_BITMAP_LADDER(float)
 #undef B200_S2N_BITMAP_LADDER
 
+// One-pass ladder for B.n <= kBitmapCols: the team bins expand, sort and
+// compress (k_esc_team) with the hash team bins' row limits; the rest is the
+// bitmap ladder.
+template<typename V>
+struct S2nEscLadder {
+    static const BinLauncher entries[];
+    static const int count;
+};
+
+#define B200_S2N_ESC_LADDER(V)                                                                \
+    template<>                                                                                \
+    const BinLauncher S2nEscLadder<V>::entries[] = {                                          \
+        {BinKind::Team, 12, 64, 256, EscLayout<V, 4, 256, 12>::bytes, "esc_team4_n12",        \
+         launch_esc<V, 4, 256, 12>},                                                          \
+        {BinKind::Team, 48, 32, 256, EscLayout<V, 8, 256, 48>::bytes, "esc_team8_n48",        \
+         launch_esc<V, 8, 256, 48>},                                                          \
+        {BinKind::Team, 192, 16, 256, EscLayout<V, 16, 256, 192>::bytes, "esc_team16_n192",   \
+         launch_esc<V, 16, 256, 192>},                                                        \
+        {BinKind::Team, 768, 8, 256, EscLayout<V, 32, 256, 768>::bytes, "esc_team32_n768",    \
+         launch_esc<V, 32, 256, 768>},                                                        \
+        S2nBitmapLadder<V>::entries[4], S2nBitmapLadder<V>::entries[5],                       \
+        S2nBitmapLadder<V>::entries[6],                                                       \
+    };                                                                                        \
+    template<>                                                                                \
+    const int S2nEscLadder<V>::count = sizeof(S2nEscLadder<V>::entries) / sizeof(BinLauncher);
+
+B200_S2N_ESC_LADDER(double)
+B200_S2N_ESC_LADDER(float)
+#undef B200_S2N_ESC_LADDER
+
 template<typename V>
 cudaError_t prepare_one() {
     cudaError_t e = cudaSuccess;
@@ -438,6 +613,10 @@ cudaError_t prepare_one() {
     B200_SMEM((k_s2n_cta<V, 512, 16384, 12288>), (CtaLayout<512, 16384, 12288>::bytes));
     B200_SMEM((k_s2n_cta<V, 1024, 43008, 32768>), (CtaLayout<1024, 43008, 32768>::bytes));
     B200_SMEM((k_s2n_bitmap<V, 1024, kBitmapCols>), (BitmapLayout<V, 1024, kBitmapCols>::bytes));
+    B200_SMEM((k_esc_team<V, 4, 256, 12>), (EscLayout<V, 4, 256, 12>::bytes));
+    B200_SMEM((k_esc_team<V, 8, 256, 48>), (EscLayout<V, 8, 256, 48>::bytes));
+    B200_SMEM((k_esc_team<V, 16, 256, 192>), (EscLayout<V, 16, 256, 192>::bytes));
+    B200_SMEM((k_esc_team<V, 32, 256, 768>), (EscLayout<V, 32, 256, 768>::bytes));
 #undef B200_SMEM
     return e;
 }
@@ -462,6 +641,24 @@ int s2n_bitmap_ladder_f64(const BinLauncher** out) {
 int s2n_bitmap_ladder_f32(const BinLauncher** out) {
     *out = S2nBitmapLadder<float>::entries;
     return S2nBitmapLadder<float>::count;
+}
+
+int s2n_esc_ladder_f64(const BinLauncher** out) {
+    *out = S2nEscLadder<double>::entries;
+    return S2nEscLadder<double>::count;
+}
+
+int s2n_esc_ladder_f32(const BinLauncher** out) {
+    *out = S2nEscLadder<float>::entries;
+    return S2nEscLadder<float>::count;
+}
+
+cudaError_t launch_esc_sample(const ProductArgs& p, int32_t m, int32_t samples,
+                              const EscLimits& lim, EscSample* out, cudaStream_t s) {
+    if (samples <= 0) return cudaSuccess;
+    k_esc_sample<<<(samples + kSampleWarps - 1) / kSampleWarps, kSampleWarps * kWarp, 0, s>>>(
+        p, m, samples, lim, out);
+    return cudaGetLastError();
 }
 
 cudaError_t s2n_prepare() {

@@ -90,6 +90,32 @@ int s2n_ladder_f32(const BinLauncher** out);
 constexpr int kBitmapCols = 1 << 20;
 int s2n_bitmap_ladder_f64(const BinLauncher** out);
 int s2n_bitmap_ladder_f32(const BinLauncher** out);
+// One-pass ladder for B.n <= kBitmapCols (key = NIP of the row): the team bins
+// expand, sort and compress; then the bitmap ladder's CTA, bitmap and global
+// bins.  Same bin count and limits as the bitmap ladder.
+int s2n_esc_ladder_f64(const BinLauncher** out);
+int s2n_esc_ladder_f32(const BinLauncher** out);
+
+// Sampled compression of the first kEscBins fill bins of a one-pass product:
+// the NIP and exact nnz of up to `samples` rows spread evenly over A, summed
+// per team bin (rows binned by NIP with `lim`; rows above the last limit are
+// skipped).  `p` needs A, B and the status word.
+constexpr int kEscBins = 4;
+constexpr int kEscSamples = 4096;
+// A team bin expands, sorts and compresses when its sampled NIP / nnz is at
+// most this (ESC sorts NIP keys where the hash bin sorts nnz; measured
+// crossovers: none up to NIP/nnz 4 for rows of <= 48 products, ~1.45 at
+// <= 192, ~1.1 at <= 768).
+constexpr double kEscMaxRatio[kEscBins] = {8.0, 8.0, 1.4, 1.1};
+struct EscLimits {
+    int32_t limit[kEscBins];
+};
+struct EscSample {
+    int64_t nip[kEscBins];
+    int64_t nnz[kEscBins];
+};
+cudaError_t launch_esc_sample(const ProductArgs& p, int32_t m, int32_t samples,
+                              const EscLimits& lim, EscSample* out, cudaStream_t s);
 // One-time per-device attribute setup (dynamic smem opt-in) for all kernels.
 cudaError_t sym1_prepare();
 cudaError_t s2n_prepare();

@@ -62,6 +62,7 @@ struct Scratch {
     int32_t* bins2;
     int32_t* fail_rows;
     int32_t* fail_count;
+    EscSample* sample;
 };
 
 struct ProfRec {
@@ -79,6 +80,7 @@ struct HostMirror {
     DevStatus status;
     int32_t fail_count;
     int32_t pad[3];
+    EscSample sample;
 };
 
 }  // namespace
@@ -89,6 +91,7 @@ struct spgemm_handle_s {
     int sm_count = 148;
     cudaStream_t side[b200::kMaxSide] = {};
     cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_sample = nullptr;  // the compression sample's side stream is done
     cudaEvent_t ev_join[b200::kMaxSide] = {};
     int nside = 4;
     // scratch (grown, never shrunk)
@@ -108,6 +111,7 @@ struct spgemm_handle_s {
     int profile = 0;
     int min_tr_bin = -1;
     int one_pass = 0;  // 0 chosen by temporary size, 1 always, 2 never (two-pass)
+    int esc = 0;  // one-pass team bins: 0 ESC where sampled compression is low, 1 always, 2 never
     // C's arrays come from the device's shared stream-ordered pool (see
     // device_pool); it keeps freed memory mapped so repeated products do not
     // re-map hundreds of MB per call.  cudaFree / cudaFreeAsync release them.
@@ -169,6 +173,7 @@ spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s, cudaStre
     const size_t o_plan1 = take(sizeof(Plan));
     const size_t o_plan2 = take(sizeof(Plan));
     const size_t o_fail_count = take(sizeof(int32_t));
+    const size_t o_sample = take(sizeof(EscSample));
     const size_t o_hist1 = take(sizeof(int32_t) * kMaxBins * nctas);
     const size_t o_hist2 = take(sizeof(int32_t) * kMaxBins * nctas);
     const size_t o_sum = take(sizeof(int64_t) * nctas);
@@ -183,6 +188,7 @@ spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s, cudaStre
     s->plan1 = reinterpret_cast<Plan*>(b + o_plan1);
     s->plan2 = reinterpret_cast<Plan*>(b + o_plan2);
     s->fail_count = reinterpret_cast<int32_t*>(b + o_fail_count);
+    s->sample = reinterpret_cast<EscSample*>(b + o_sample);
     s->hist1 = reinterpret_cast<int32_t*>(b + o_hist1);
     s->hist2 = reinterpret_cast<int32_t*>(b + o_hist2);
     s->cta_sum = reinterpret_cast<int64_t*>(b + o_sum);
@@ -256,7 +262,10 @@ spgemm_status status_to_error(const DevStatus& st) {
 }
 
 spgemm_status sync_mirror(spgemm_handle_s* h, cudaStream_t stream, const Plan* plan,
-                          const Scratch& s) {
+                          const Scratch& s, bool with_sample = false) {
+    if (with_sample)
+        B200_TRY(cudaMemcpyAsync(&h->mirror->sample, s.sample, sizeof(EscSample),
+                                 cudaMemcpyDeviceToHost, stream));
     B200_TRY(cudaMemcpyAsync(&h->mirror->plan, plan, sizeof(Plan), cudaMemcpyDeviceToHost,
                              stream));
     B200_TRY(cudaMemcpyAsync(&h->mirror->status, s.status, sizeof(DevStatus),
@@ -514,7 +523,9 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         int32_t* off = nullptr;
         int32_t* tmp_col = nullptr;
         void* tmp_val = nullptr;
+        bool sampling = false;  // the compression sample may still read A and B
         auto release = [&]() {
+            if (sampling) cudaStreamWaitEvent(stream, h->ev_sample, 0);
             if (off) cudaFreeAsync(off, stream);
             if (tmp_col) cudaFreeAsync(tmp_col, stream);
             if (tmp_val) cudaFreeAsync(tmp_val, stream);
@@ -542,7 +553,32 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         B200_ONE_CUDA(cudaMemcpyAsync(off, c_rpt, sizeof(int32_t) * size_t(m),
                                       cudaMemcpyDeviceToDevice, stream),
                       "copy NIP per row");
+        // B.n <= 2^20: team bins may expand, sort and compress instead of
+        // hashing (same limits, so the binning does not depend on it)
+        BinLauncher one_fil[16];
+        for (int b = 0; b < nfil && b < 16; b++) one_fil[b] = fil[b];
+        const bool esc_ok = narrow && h->esc != 2;
+        const bool esc_sampled = esc_ok && h->esc == 0;
         const Ladder ladf = make_ladder(fil, nfil, h->min_num_bin);
+        if (esc_sampled) {
+            // the compression sample reads A and B only: it runs on a side
+            // stream beside the fill binning and joins before the host sync
+            EscLimits el{};
+            for (int b = 0; b < kEscBins; b++) el.limit[b] = fil[b].limit;
+            const int32_t samples = std::min<int32_t>(m, kEscSamples);
+            cudaStream_t side = h->side[0];
+            B200_ONE_CUDA(cudaMemsetAsync(s.sample, 0, sizeof(EscSample), stream),
+                          "reset the compression sample");
+            B200_ONE_CUDA(cudaEventRecord(h->ev_fork, stream), "fork the sample stream");
+            B200_ONE_CUDA(cudaStreamWaitEvent(side, h->ev_fork, 0), "fork the sample stream");
+            const spgemm_status st_sample =
+                timed(h, "esc_sample", 2, -1, samples, side,
+                      [&](cudaStream_t ss) { return launch_esc_sample(pa, m, samples, el, s.sample, ss); });
+            // recorded whatever the launch returned, so an error path can wait on it
+            B200_ONE_CUDA(cudaEventRecord(h->ev_sample, side), "join the sample stream");
+            sampling = true;
+            B200_ONE(st_sample);
+        }
         B200_ONE(timed(h, "nip_fill_hist", 2, -1, m, stream, [&](cudaStream_t ss) {
             return launch_nnz_hist(off, m, s.hist2, s.cta_sum, s.plan2, ladf, ss);
         }));
@@ -564,10 +600,28 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
                                               stream),
                       "allocate the one-pass values");
         mark(2);
-        B200_ONE(sync_mirror(h, stream, s.plan2, s));
+        if (esc_sampled) {
+            B200_ONE_CUDA(cudaStreamWaitEvent(stream, h->ev_sample, 0), "join the sample stream");
+            sampling = false;
+        }
+        B200_ONE(sync_mirror(h, stream, s.plan2, s, esc_sampled));
         mark(3);
         B200_ONE(status_to_error(h->mirror->status));
         const Plan pf = h->mirror->plan;
+        if (esc_ok) {
+            const BinLauncher* esc = nullptr;
+            const int nesc = sizeof(V) == 8 ? s2n_esc_ladder_f64(&esc) : s2n_esc_ladder_f32(&esc);
+            const EscSample& es = h->mirror->sample;
+            for (int b = 0; b < kEscBins && b < nesc && b < nfil; b++) {
+                const bool use = !esc_sampled || (es.nnz[b] > 0 &&
+                                                  static_cast<double>(es.nip[b]) <=
+                                                      kEscMaxRatio[b] * static_cast<double>(es.nnz[b]));
+                if (use) {
+                    one_fil[b] = esc[b];
+                    h->info.esc_mask |= 1 << b;
+                }
+            }
+        }
         for (int b = 0; b < nfil && b < 16; b++) h->info.num_bin_rows[b] = pf.bin_size[b];
         pa.c_rpt = off;
         pa.c_col = tmp_col;
@@ -580,7 +634,7 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
             pa.nmaps = nmaps;
         }
         mark(4);
-        B200_ONE(launch_bins(h, fil, nfil, 3, pf, s.bins2, pa, stream));
+        B200_ONE(launch_bins(h, one_fil, nfil, 3, pf, s.bins2, pa, stream));
         // row pointer from the counts: a one-bin pass with the scan, into the
         // count binning's plan (reset: its max and overflow only ever grow)
         B200_ONE_CUDA(cudaMemsetAsync(s.plan1, 0, sizeof(Plan), stream), "reset a plan");
@@ -1628,6 +1682,7 @@ spgemm_status spgemm_create(spgemm_handle_t* handle, int device) {
         B200_TRY(cudaEventCreateWithFlags(&h->ev_join[i], cudaEventDisableTiming));
     }
     B200_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+    B200_TRY(cudaEventCreateWithFlags(&h->ev_sample, cudaEventDisableTiming));
     B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&h->mirror), sizeof(HostMirror)));
     if (spgemm_status st = device_pool(dev, &h->pool); st != SPGEMM_OK) return st;
     *handle = h;
@@ -1643,6 +1698,7 @@ spgemm_status spgemm_destroy(spgemm_handle_t h) {
         if (h->ev_join[i]) cudaEventDestroy(h->ev_join[i]);
     }
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_sample) cudaEventDestroy(h->ev_sample);
     if (h->scratch) cudaFree(h->scratch);
     if (h->bitmaps) cudaFree(h->bitmaps);
     if (h->in_buf) cudaFree(h->in_buf);
@@ -1914,6 +1970,10 @@ spgemm_status spgemm_set_option(spgemm_handle_t h, spgemm_option opt, int64_t va
                 return fail(SPGEMM_ERR_INVALID_ARG, "one-pass must be 0, 1 or 2");
             h->one_pass = static_cast<int>(value);
             return SPGEMM_OK;
+        case SPGEMM_OPT_ESC:
+            if (value < 0 || value > 2) return fail(SPGEMM_ERR_INVALID_ARG, "ESC must be 0, 1 or 2");
+            h->esc = static_cast<int>(value);
+            return SPGEMM_OK;
     }
     return fail(SPGEMM_ERR_INVALID_ARG, "unknown option");
 }
@@ -1929,6 +1989,7 @@ spgemm_status spgemm_get_option(spgemm_handle_t h, spgemm_option opt, int64_t* v
         case SPGEMM_OPT_PROFILE: *value = h->profile; return SPGEMM_OK;
         case SPGEMM_OPT_MIN_TRANSPOSE_BIN: *value = h->min_tr_bin; return SPGEMM_OK;
         case SPGEMM_OPT_ONE_PASS: *value = h->one_pass; return SPGEMM_OK;
+        case SPGEMM_OPT_ESC: *value = h->esc; return SPGEMM_OK;
     }
     return fail(SPGEMM_ERR_INVALID_ARG, "unknown option");
 }
@@ -1947,8 +2008,10 @@ spgemm_status spgemm_ladder_info(spgemm_handle_t h, int which, int dtype_bytes, 
         nb = dtype_bytes == 8 ? s2n_bitmap_ladder_f64(&l) : s2n_bitmap_ladder_f32(&l);
     } else if (which == 3) {
         nb = dtype_bytes == 8 ? transpose_ladder_f64(&l) : transpose_ladder_f32(&l);
+    } else if (which == 4) {
+        nb = dtype_bytes == 8 ? s2n_esc_ladder_f64(&l) : s2n_esc_ladder_f32(&l);
     } else {
-        return fail(SPGEMM_ERR_INVALID_ARG, "ladder id must be 0..3");
+        return fail(SPGEMM_ERR_INVALID_ARG, "ladder id must be 0..4");
     }
     *n_bins = nb;
     for (int i = 0; i < 16; i++) limits[i] = i < nb ? l[i].limit : 0;

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define SPGEMM_ABI_VERSION 3
+#define SPGEMM_ABI_VERSION 4
 
 #if defined(__GNUC__)
 #define SPGEMM_API __attribute__((visibility("default")))
@@ -100,6 +100,7 @@ typedef struct spgemm_info {
      * fill kernels queued, final sync done (unused entries 0) */
     float phase_us[8];
     int32_t one_pass;        /* 1: C's row sizes came from the one-pass fill */
+    int32_t esc_mask;        /* bit b: one-pass team bin b expanded, sorted and compressed */
 } spgemm_info;
 
 /* ---- lifecycle ------------------------------------------------------------ */
@@ -189,7 +190,14 @@ typedef enum spgemm_option {
      * kernels give each row's exact nnz, the fill writes C in place.  One
      * pass: rows are filled into NIP-sized slots while their nnz is counted,
      * then compacted into C -- no count kernels, one more copy of C. */
-    SPGEMM_OPT_ONE_PASS = 8
+    SPGEMM_OPT_ONE_PASS = 8,
+    /* One-pass products with B.n <= 2^20: whether the four team fill bins
+     * (rows of up to 12, 48, 192 and 768 intermediate products) expand, sort
+     * and compress -- stage every product, sort by column, sum each column's
+     * run in product order -- instead of hashing.  0 (default): per bin,
+     * when the NIP / nnz of up to 64 sampled rows of the bin is at most 1.5;
+     * 1: always; 2: never.  spgemm_info.esc_mask says which bins did. */
+    SPGEMM_OPT_ESC = 9
 } spgemm_option;
 
 SPGEMM_API spgemm_status spgemm_set_option(spgemm_handle_t handle, spgemm_option option, int64_t value);
@@ -214,7 +222,9 @@ SPGEMM_API spgemm_status spgemm_last_profile(spgemm_handle_t handle, spgemm_kern
  * key -- NIP for the count ladder, nnz for the fill ladders -- is <= limit).
  * which: 0 count ladder; 1 fill ladder used when B.n > 2^20; 2 fill ladder
  * used when B.n <= 2^20 (its large rows use a shared-memory bitmap);
- * 3 row-sort ladder of spgemm_transpose_* (key = length of a row of A^T). */
+ * 3 row-sort ladder of spgemm_transpose_* (key = length of a row of A^T);
+ * 4 one-pass fill ladder used when B.n <= 2^20 (key = NIP; its team bins
+ * expand, sort and compress, see SPGEMM_OPT_ESC). */
 SPGEMM_API spgemm_status spgemm_ladder_info(spgemm_handle_t handle, int which,
                                  int dtype_bytes, int* n_bins, int64_t* limits /*[16]*/);
 

@@ -25,7 +25,7 @@ def test_library_exports_every_symbol(native_lib):
 
 
 def test_status_strings_and_version(native_lib):
-    assert native_lib.spgemm_abi_version() == 3
+    assert native_lib.spgemm_abi_version() == 4
     assert native_lib.spgemm_status_string(0) == b"SPGEMM_OK"
     assert native_lib.spgemm_status_string(4) == b"SPGEMM_ERR_OVERFLOW"
 
@@ -53,3 +53,20 @@ def test_ladders_are_monotone(native_lib):
             assert nb.value >= 5
             assert all(x <= y for x, y in zip(vals, vals[1:]))
             assert vals[-1] == 2**31 - 1
+
+
+def test_esc_ladder_matches_bitmap_ladder(native_lib):
+    """The one-pass ladder with expand-sort-compress team bins routes rows
+    exactly like the bitmap ladder it replaces them in (same bins, same
+    limits), so SPGEMM_OPT_ESC changes kernels, never the binning."""
+    def limits(which, nbytes):
+        nb = C.c_int()
+        lim = (C.c_int64 * 16)()
+        assert native_lib.spgemm_ladder_info(None, which, nbytes, C.byref(nb), lim) == 0
+        return list(lim)[: nb.value]
+    for nbytes in (4, 8):
+        assert limits(4, nbytes) == limits(2, nbytes)
+        assert limits(4, nbytes)[:4] == [12, 48, 192, 768]
+    nb = C.c_int()
+    lim = (C.c_int64 * 16)()
+    assert native_lib.spgemm_ladder_info(None, 5, 8, C.byref(nb), lim) != 0
