@@ -282,21 +282,33 @@ __global__ __launch_bounds__(THREADS) void k_s2n_cta(ProductArgs p) {
 // Bitmap bin (B.n <= kBitmapCols): the row's hash table is the identity hash
 // over B's columns, one BIT per column, in shared memory (128 KB for 2^20
 // columns).  atomicOr fills it; the set bits read in word order are the sorted
-// column list, so no sort is needed.  Extraction: each warp owns a contiguous
-// run of words; warp totals are scanned across the CTA, then each warp scans
-// its 32-word chunks with shuffles, writes its columns to C.col and records
-// the rank of every 8-word block's first bit.  The bitmap stays intact, so a
-// key's position in the row is its rank -- the block's rank plus the set bits
-// before it in at most 8 words, all independent reads -- instead of a binary
-// search; values accumulate with global reductions into C.val.  Shared memory
-// does not grow with the row, so every row of the bin's range fits.
+// column list, so no sort is needed.  A summary bitmap holds one bit per
+// bitmap word that has any bit set (set by the product that set the word's
+// first bit), so counting, extracting and clearing visit only the row's
+// non-empty words: the cost of a row follows its products, not B.n.
+//
+// The kernel is persistent: one CTA per SM (the bitmap takes most of its
+// shared memory) clears the bitmap once and then takes rows blockIdx.x,
+// blockIdx.x + gridDim.x, ...  Thread t owns summary word t, i.e. bitmap
+// words [32t, 32t + 32) = four 8-word blocks.  Per row: fill; each thread
+// counts the set bits of its non-empty words; a block scan gives every
+// thread's first position, from which it writes its columns to C.col and
+// records the rank of each of its blocks' first bit.  The bitmap stays
+// intact, so a key's position in the row is its rank -- the block's rank plus
+// the set bits before it in at most 8 words, all independent reads --
+// instead of a binary search; values accumulate with global reductions into
+// C.val.  Then each thread clears its non-empty words and summary word.
 constexpr int kBitmapWords = kBitmapCols / 32;
+constexpr int kSummaryWords = kBitmapWords / 32;
 
 template<typename V, int THREADS, int CAP>
 struct BitmapLayout {
     static constexpr size_t bm_bytes = sizeof(uint32_t) * kBitmapWords;
+    static constexpr size_t summary_bytes = sizeof(uint32_t) * kSummaryWords;
     static constexpr size_t rank_bytes = sizeof(int32_t) * (kBitmapWords / 8);
-    static constexpr size_t bytes = bm_bytes + rank_bytes + sizeof(CtaScratch<THREADS>);
+    static constexpr size_t bytes =
+        bm_bytes + summary_bytes + rank_bytes + sizeof(CtaScratch<THREADS>);
+    static_assert(kSummaryWords == THREADS, "one summary word per thread");
 };
 
 template<typename V, int THREADS, int CAP>
@@ -305,87 +317,79 @@ __global__ __launch_bounds__(THREADS) void k_s2n_bitmap(ProductArgs p) {
     constexpr int NW = THREADS / kWarp;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* bm = reinterpret_cast<uint32_t*>(smem_raw);
-    int32_t* block_rank = reinterpret_cast<int32_t*>(smem_raw + L::bm_bytes);
-    auto& sc = *reinterpret_cast<CtaScratch<THREADS>*>(smem_raw + L::bm_bytes + L::rank_bytes);
+    uint32_t* summary = reinterpret_cast<uint32_t*>(smem_raw + L::bm_bytes);
+    int32_t* block_rank = reinterpret_cast<int32_t*>(smem_raw + L::bm_bytes + L::summary_bytes);
+    auto& sc = *reinterpret_cast<CtaScratch<THREADS>*>(smem_raw + L::bm_bytes +
+                                                        L::summary_bytes + L::rank_bytes);
     const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int w = tid >> 5;
-    const int row = p.rows[blockIdx.x];
-    const int c0 = p.c_rpt[row];
-    // the row's exact nnz, or in one-pass mode its NIP (an upper bound)
-    const int bound = p.c_rpt[row + 1] - c0;
     const int words = (p.n_cols + 31) >> 5;
-    if (bound > CAP || words > kBitmapWords) {
-        if (tid == 0) report(p.status, kStCapacity, row, bound);
+    if (words > kBitmapWords) {
+        if (tid == 0 && blockIdx.x < p.nrows) report(p.status, kStCapacity, p.rows[blockIdx.x], 0);
         return;
     }
     for (int i = tid; i < words; i += THREADS) bm[i] = 0u;
+    summary[tid] = 0u;
     __syncthreads();
-    const int a0 = p.a_rpt[row];
-    const int a1 = p.a_rpt[row + 1];
-    cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int) {
-        const int32_t key = __ldg(p.b_col + qb);
-        atomicOr(bm + (key >> 5), 1u << (key & 31));
-    });
-    // warp w reads words [w0, w1)
-    const int seg = (words + NW - 1) / NW;
-    const int w0 = min(words, w * seg);
-    const int w1 = min(words, w0 + seg);
-    int cnt = 0;
-    for (int i = w0 + lane; i < w1; i += kWarp) cnt += __popc(bm[i]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-    if (lane == 0) sc.warp_tot[w] = cnt;
-    __syncthreads();
-    int base = 0;
-    int total = 0;
-#pragma unroll
-    for (int k = 0; k < NW; k++) {
-        const int t = sc.warp_tot[k];
-        base += k < w ? t : 0;
-        total += t;
-    }
-    int32_t* cols = p.c_col + c0;
-    for (int c = w0; c < w1; c += kWarp) {
-        const int i = c + lane;
-        uint32_t word = i < w1 ? bm[i] : 0u;
-        const int pc = __popc(word);
-        int inc = pc;
-#pragma unroll
-        for (int o = 1; o < kWarp; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += t;
+    const int w0 = tid * 32;  // this thread's bitmap words [w0, w0 + 32)
+    for (int rid = blockIdx.x; rid < p.nrows; rid += gridDim.x) {
+        const int row = p.rows[rid];
+        const int c0 = p.c_rpt[row];
+        // the row's exact nnz, or in one-pass mode its NIP (an upper bound)
+        const int bound = p.c_rpt[row + 1] - c0;
+        if (bound > CAP) {  // uniform over the CTA
+            if (tid == 0) report(p.status, kStCapacity, row, bound);
+            continue;
         }
-        int pos = base + inc - pc;
-        if (i < w1 && (i & 7) == 0) block_rank[i >> 3] = pos;
-        while (word != 0u) {
-            const int b = __ffs(word) - 1;
-            if (pos < bound) cols[pos] = i * 32 + b;
-            pos++;
-            word &= word - 1u;
-        }
-        base += __shfl_sync(0xffffffffu, inc, kWarp - 1);
-    }
-    int nnz = bound;
-    if (p.row_nnz != nullptr) {  // one-pass: the count is the row's nnz
-        nnz = total <= bound ? total : bound;
-        if (tid == 0) p.row_nnz[row] = nnz;
-    } else if (total != nnz && tid == 0) {
-        report(p.status, kStCapacity, row, total);
-    }
-    V* out = static_cast<V*>(p.c_val) + c0;
-    for (int i = tid; i < nnz; i += THREADS) out[i] = V(0);
-    __syncthreads();
-    cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int ai) {
-        const int32_t key = __ldg(p.b_col + qb);
-        const int wi = key >> 5;
-        const int w8 = wi & ~7;
-        int rank = block_rank[wi >> 3] + __popc(bm[wi] & ((1u << (key & 31)) - 1u));
+        const int a0 = p.a_rpt[row];
+        const int a1 = p.a_rpt[row + 1];
+        cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int) {
+            const int32_t key = __ldg(p.b_col + qb);
+            const int wi = key >> 5;
+            if (atomicOr(bm + wi, 1u << (key & 31)) == 0u)
+                atomicOr(summary + (wi >> 5), 1u << (wi & 31));
+        });
+        const uint32_t sw = summary[tid];
+        int cnt = 0;
+        for (uint32_t m = sw; m != 0u; m &= m - 1u) cnt += __popc(bm[w0 + __ffs(m) - 1]);
+        const int inc = block_inclusive_scan<THREADS>(cnt, sc.warp_tot);
+        const int total = sc.warp_tot[NW - 1];
+        int pos = inc - cnt;
+        int32_t* cols = p.c_col + c0;
 #pragma unroll
-        for (int t = 0; t < 7; t++)
-            if (w8 + t < wi) rank += __popc(bm[w8 + t]);
-        if (rank < nnz) atomicAdd(out + rank, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
-    });
+        for (int bb = 0; bb < 4; bb++) {
+            block_rank[(w0 >> 3) + bb] = pos;
+            for (uint32_t m = (sw >> (8 * bb)) & 0xffu; m != 0u; m &= m - 1u) {
+                const int wi = w0 + 8 * bb + __ffs(m) - 1;
+                for (uint32_t word = bm[wi]; word != 0u; word &= word - 1u) {
+                    if (pos < bound) cols[pos] = wi * 32 + __ffs(word) - 1;
+                    pos++;
+                }
+            }
+        }
+        int nnz = bound;
+        if (p.row_nnz != nullptr) {  // one-pass: the count is the row's nnz
+            nnz = total <= bound ? total : bound;
+            if (tid == 0) p.row_nnz[row] = nnz;
+        } else if (total != nnz && tid == 0) {
+            report(p.status, kStCapacity, row, total);
+        }
+        V* out = static_cast<V*>(p.c_val) + c0;
+        for (int i = tid; i < nnz; i += THREADS) out[i] = V(0);
+        __syncthreads();
+        cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int ai) {
+            const int32_t key = __ldg(p.b_col + qb);
+            const int wi = key >> 5;
+            const int w8 = wi & ~7;
+            int rank = block_rank[wi >> 3] + __popc(bm[wi] & ((1u << (key & 31)) - 1u));
+#pragma unroll
+            for (int t = 0; t < 7; t++)
+                if (w8 + t < wi) rank += __popc(bm[w8 + t]);
+            if (rank < nnz) atomicAdd(out + rank, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
+        });
+        for (uint32_t m = sw; m != 0u; m &= m - 1u) bm[w0 + __ffs(m) - 1] = 0u;
+        summary[tid] = 0u;
+        __syncthreads();
+    }
 }
 
 // Global bin: a bitmap per row in flight (global scratch, B.n bits per CTA);
@@ -498,8 +502,11 @@ cudaError_t launch_cta(const ProductArgs& p, cudaStream_t s) {
 
 template<typename V, int THREADS, int CAP>
 cudaError_t launch_bitmap(const ProductArgs& p, cudaStream_t s) {
-    k_s2n_bitmap<V, THREADS, CAP>
-        <<<p.nrows, THREADS, BitmapLayout<V, THREADS, CAP>::bytes, s>>>(p);
+    // persistent: one CTA per SM at most (the bitmap takes most of an SM's
+    // shared memory)
+    const int sms = p.sm_count > 0 ? p.sm_count : 148;
+    const int grid = p.nrows < sms ? p.nrows : sms;
+    k_s2n_bitmap<V, THREADS, CAP><<<grid, THREADS, BitmapLayout<V, THREADS, CAP>::bytes, s>>>(p);
     return cudaGetLastError();
 }
 

@@ -61,6 +61,8 @@ struct ProductArgs {
     // bound); the kernel writes the row's exact nnz here (nullptr: c_rpt is
     // C's exact row pointer)
     int32_t* row_nnz;
+    // SMs of the device (persistent kernels size their grid by it; 0: 148)
+    int32_t sm_count;
 };
 
 enum class BinKind : int { Team = 0, Cta = 1, Cluster = 2, Global = 3 };

@@ -503,6 +503,7 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     pa.fail_rows = s.fail_rows;
     pa.fail_count = s.fail_count;
     pa.words = (static_cast<int64_t>(n) + 31) / 32;
+    pa.sm_count = h->sm_count;
 
     // ---- one-pass fill: no count phase ------------------------------------
     // Rows are binned by NIP (an upper bound of their nnz) on the fill ladder
