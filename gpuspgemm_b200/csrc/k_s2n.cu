@@ -344,6 +344,10 @@ __global__ __launch_bounds__(THREADS) void k_s2n_bitmap(ProductArgs p) {
         const int a1 = p.a_rpt[row + 1];
         cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int) {
             const int32_t key = __ldg(p.b_col + qb);
+            if (static_cast<uint32_t>(key) >= static_cast<uint32_t>(p.n_cols)) {
+                report(p.status, kStBadInput, row, key);  // outside the bitmap
+                return;
+            }
             const int wi = key >> 5;
             if (atomicOr(bm + wi, 1u << (key & 31)) == 0u)
                 atomicOr(summary + (wi >> 5), 1u << (wi & 31));
@@ -378,6 +382,7 @@ __global__ __launch_bounds__(THREADS) void k_s2n_bitmap(ProductArgs p) {
         __syncthreads();
         cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int ai) {
             const int32_t key = __ldg(p.b_col + qb);
+            if (static_cast<uint32_t>(key) >= static_cast<uint32_t>(p.n_cols)) return;
             const int wi = key >> 5;
             const int w8 = wi & ~7;
             int rank = block_rank[wi >> 3] + __popc(bm[wi] & ((1u << (key & 31)) - 1u));

@@ -293,6 +293,26 @@ def test_esc_sums_in_oracle_order(handle, oracle_mod, dtype):
         handle.set_option(N.OPT_ESC, 0)
 
 
+@pytest.mark.parametrize("passes", [1, 2])
+def test_bitmap_bin_back_to_back(handle, oracle_mod, passes):
+    """Every row through the bitmap bin, whose persistent CTAs clear only the
+    bitmap words a row set before taking the next row: back-to-back products
+    of different structures and value types all match the oracle."""
+    from gpuspgemm_b200 import _native as N
+    assert len(handle.ladder(2, 8)) == 7
+    handle.set_option(N.OPT_MIN_NUM_BIN, 5)
+    handle.set_option(N.OPT_ONE_PASS, passes)
+    try:
+        for seed, dtype in [(61, np.float64), (62, np.float64), (63, np.float32), (61, np.float64)]:
+            A = G.power_law(4000, 2.0, 400, seed=seed)
+            C = gpu_product(A, A, handle, dtype)
+            check(oracle_mod, A, A, C, dtype, f"bitmap_back_to_back_{seed}_pass{passes}",
+                  positive=True)
+    finally:
+        handle.set_option(N.OPT_MIN_NUM_BIN, -1)
+        handle.set_option(N.OPT_ONE_PASS, 0)
+
+
 def test_one_pass_chosen_and_equal_to_two_pass(handle, oracle_mod):
     """By default a product whose temporaries fit runs one pass; its C equals
     the two-pass C in structure, and both match the oracle."""
