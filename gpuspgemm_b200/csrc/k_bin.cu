@@ -60,26 +60,39 @@ __global__ __launch_bounds__(kBinThreads) void k_nip_hist(
             s1 = a_rpt[r + 1];
         }
         const int len = s1 - s0;
-        const int maxlen = __reduce_max_sync(0xffffffffu, len);
         long long nip = 0;
-        if (maxlen >= kWarp) {
-            // a warp per row when any row of the group is long (setup.cuh:52-75)
-            for (int i = 0; i < kWarp; i++) {
-                const int rs = __shfl_sync(0xffffffffu, s0, i);
-                const int re = __shfl_sync(0xffffffffu, s1, i);
-                long long part = 0;
-                for (int p = rs + lane; p < re; p += kWarp) {
-                    const int c = __ldg(a_col + p);
-                    part += __ldg(b_rpt + c + 1) - __ldg(b_rpt + c);
-                }
-                part = warp_sum_ll(part);
-                if (lane == i) nip = part;
-            }
-        } else {
+        // short rows: a lane each, all at once; long rows (>= 32 entries): the
+        // whole warp, one after another (setup.cuh:52-75 gives the warp every
+        // row of a group that holds a long one)
+        if (len < kWarp) {
+#pragma unroll 4
             for (int p = s0; p < s1; p++) {
                 const int c = __ldg(a_col + p);
                 nip += __ldg(b_rpt + c + 1) - __ldg(b_rpt + c);
             }
+        }
+        for (unsigned longm = __ballot_sync(0xffffffffu, len >= kWarp); longm != 0u;
+             longm &= longm - 1u) {
+            const int i = __ffs(longm) - 1;
+            const int rs = __shfl_sync(0xffffffffu, s0, i);
+            const int re = __shfl_sync(0xffffffffu, s1, i);
+            // 8 entries per lane in flight: all their columns first, then all
+            // the B-row bounds (the longest rows set the kernel's duration)
+            constexpr int U = 8;
+            long long part = 0;
+            for (int p0 = rs + lane; p0 < re; p0 += U * kWarp) {
+                int c[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int p = p0 + u * kWarp;
+                    c[u] = p < re ? __ldg(a_col + p) : -1;
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++)
+                    if (c[u] >= 0) part += __ldg(b_rpt + c[u] + 1) - __ldg(b_rpt + c[u]);
+            }
+            part = warp_sum_ll(part);
+            if (lane == i) nip = part;
         }
         if (r < m) {
             int32_t key;
@@ -290,18 +303,24 @@ __global__ __launch_bounds__(kBinThreads) void k_bin_scatter(
 // Row r's entries sit at [off[r], off[r] + nnz_r) of the temporary arrays (its
 // NIP-sized slot); copy them to [rpt[r], rpt[r+1]) of C.  One CTA per chunk
 // of kCompactRows rows stages the chunk's row pointers and slot offsets in
-// shared memory and walks the chunk's OUTPUT entries with consecutive threads
-// (coalesced writes; reads coalesced within rows), finding each entry's row
-// by a binary search in shared memory.
+// shared memory.  Its warps take tiles of 32 x kCompactUnroll consecutive
+// OUTPUT entries; lane l copies entries tile + 32k + l (coalesced writes;
+// reads coalesced within rows).  An entry's row is found by one binary search
+// per tile and lane, then by stepping the row forward from one of the lane's
+// entries to the next -- unless the chunk's rows average fewer than
+// kCompactStepMin entries, where every entry does its own binary search.
 constexpr int kCompactRows = 256;
 constexpr int kCompactThreads = 256;
-constexpr int kCompactUnroll = 4;  // independent entries per thread in flight
+constexpr int kCompactUnroll = 8;    // entries per lane and tile, in flight together
+constexpr int kCompactStepMin = 16;  // mean row length from which rows are stepped
 
 template<typename W>
 __global__ __launch_bounds__(kCompactThreads) void k_compact_rows(
     const int32_t* __restrict__ off, const int32_t* __restrict__ rpt, int32_t m,
     const int32_t* __restrict__ tmp_col, const W* __restrict__ tmp_val,
     int32_t* __restrict__ col, W* __restrict__ val) {
+    constexpr int NW = kCompactThreads / kWarp;
+    constexpr int U = kCompactUnroll;
     __shared__ int32_t s_rpt[kCompactRows + 1];
     __shared__ int32_t s_off[kCompactRows];
     const int r0 = blockIdx.x * kCompactRows;
@@ -313,33 +332,43 @@ __global__ __launch_bounds__(kCompactThreads) void k_compact_rows(
     __syncthreads();
     const int j0 = s_rpt[0];
     const int j1 = s_rpt[nr];
-    for (int base = j0 + threadIdx.x; base < j1; base += kCompactThreads * kCompactUnroll) {
-        int src[kCompactUnroll];
+    const bool step = (j1 - j0) >= kCompactStepMin * nr;  // uniform over the CTA
+    // the last row i of the chunk with s_rpt[i] <= j
+    auto search = [&](int j) {
+        int lo = 0;
+        int len = nr;
+        while (len > 1) {
+            const int half = len >> 1;
+            lo = s_rpt[lo + half] <= j ? lo + half : lo;
+            len -= half;
+        }
+        return lo;
+    };
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    for (int t0 = j0 + w * kWarp * U; t0 < j1; t0 += NW * kWarp * U) {
+        int src[U];
+        int lo = search(min(t0 + lane, j1 - 1));
 #pragma unroll
-        for (int u = 0; u < kCompactUnroll; u++) {
-            const int j = base + u * kCompactThreads;
-            // the last row i of the chunk with s_rpt[i] <= j
-            int lo = 0;
-            int len = nr;
-            while (len > 1) {
-                const int half = len >> 1;
-                lo = s_rpt[lo + half] <= j ? lo + half : lo;
-                len -= half;
+        for (int u = 0; u < U; u++) {
+            const int j = min(t0 + u * kWarp + lane, j1 - 1);
+            if (step) {
+                while (s_rpt[lo + 1] <= j) lo++;
+            } else {
+                lo = search(j);
             }
             src[u] = s_off[lo] + (j - s_rpt[lo]);
         }
-        int32_t c[kCompactUnroll];
-        W v[kCompactUnroll];
+        int32_t c[U];
+        W v[U];
 #pragma unroll
-        for (int u = 0; u < kCompactUnroll; u++) {
-            if (base + u * kCompactThreads < j1) {
-                c[u] = __ldg(tmp_col + src[u]);
-                v[u] = __ldg(tmp_val + src[u]);
-            }
+        for (int u = 0; u < U; u++) {
+            c[u] = __ldg(tmp_col + src[u]);
+            v[u] = __ldg(tmp_val + src[u]);
         }
 #pragma unroll
-        for (int u = 0; u < kCompactUnroll; u++) {
-            const int j = base + u * kCompactThreads;
+        for (int u = 0; u < U; u++) {
+            const int j = t0 + u * kWarp + lane;
             if (j < j1) {
                 col[j] = c[u];
                 val[j] = v[u];
