@@ -51,6 +51,11 @@ TRAFFIC_PER_ALG_BYTE = {
     "s2n_team16_t256": 10184960 / 16517676,
     "s2n_team32_t1024": 10851840 / 20804236,
     "s2n_cta256_t4096": 11505152 / 24898604,
+    # one-pass expand-sort-compress bins (rows keyed by NIP), same n = 200k case
+    "esc_team4_n12": 9732864 / 14947704,
+    "esc_team8_n48": 8819456 / 11855028,
+    "esc_team16_n192": 9604608 / 16511032,
+    "esc_team32_n768": 10614272 / 20784028,
 }
 
 
@@ -360,9 +365,12 @@ def run_ours(args, rank, world, local_rank):
     nz = deg > 0
     nip_rows[nz] = np.add.reduceat(contrib, A.rpt[:-1][nz])
     nnz_rows = np.diff(c_rpt).astype(np.int64)
-    if phase == 3:
+    if name == "compact_rows":
+        lim, keys = None, None
+    elif phase == 3:
         lim = h.ladder(2 if A.n <= (1 << 20) else 1, s_bytes)
-        keys = nnz_rows
+        # one-pass products bin their fill rows by NIP, two-pass ones by nnz
+        keys = nip_rows if info["one_pass"] else nnz_rows
         numeric, write_c = True, True
     elif phase == 1:
         lim = h.ladder(0)
@@ -374,6 +382,8 @@ def run_ours(args, rank, world, local_rank):
         bins = bin_rows(keys, lim)
         rows = np.nonzero((keys > 0) & (bins == b))[0]
         alg_bytes = rows_bytes(A, rows, nnz_rows[rows], s_bytes, numeric, write_c)
+    elif name == "compact_rows":
+        alg_bytes = 8 * A.m + 2 * (4 + s_bytes) * int(nnz_rows.sum())  # C read and written
     else:
         alg_bytes = 8 * A.m  # binning passes: row pointers / keys in and out
     peaks = json.loads(PEAKS_FILE.read_text()) if PEAKS_FILE.exists() else {}

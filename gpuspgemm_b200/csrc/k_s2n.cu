@@ -172,11 +172,13 @@ __global__ __launch_bounds__(THREADS) void k_esc_team(ProductArgs p) {
 // Compression of the team bins, sampled: `samples` rows spread evenly over
 // A are counted exactly (one warp per row, a 1024-slot shared hash set) when
 // their NIP is at most the last team bin's limit, and their NIP and nnz are
-// summed per team bin (binned by NIP with the ladder's limits).  It needs A
-// and B only, so it runs beside the fill binning; the host reads the sums
-// with the binning plan and lets a team bin expand-sort-compress only when
-// its rows repeat few columns: ESC sorts every product, the hash bins only
-// the distinct columns.
+// summed per team bin (binned by NIP with the ladder's limits); the NIP of
+// the longer sampled rows is summed apart.  It needs A and B only, so it runs
+// on a side stream beside the NIP pass; the host reads the sums with the NIP
+// plan.  They choose one pass or two (rows above the team bins that repeat
+// many columns fill small nnz-sized tables only in two passes) and let a
+// team bin expand-sort-compress only when its rows repeat few columns: ESC
+// sorts every product, the hash bins only the distinct columns.
 constexpr int kSampleWarps = 8;
 constexpr int kSampleSlots = 1024;
 
@@ -193,7 +195,19 @@ __global__ __launch_bounds__(kSampleWarps * kWarp) void k_esc_sample(ProductArgs
     const int a0 = p.a_rpt[row];
     const int a1 = p.a_rpt[row + 1];
     const int cap = lim.limit[kEscBins - 1];
-    if (a1 - a0 > cap) return;  // more products than the team bins take
+    auto count_nip = [&](int64_t v, bool above) {
+        if (lane == 0) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(&out->nip_seen),
+                      static_cast<unsigned long long>(v));
+            if (above)
+                atomicAdd(reinterpret_cast<unsigned long long*>(&out->nip_above),
+                          static_cast<unsigned long long>(v));
+        }
+    };
+    if (a1 - a0 > cap) {  // more products than the team bins take (>= a1 - a0)
+        count_nip(a1 - a0, true);
+        return;
+    }
     int nip = 0;
     for (int e = a0 + lane; e < a1; e += kWarp) {
         const int c = __ldg(p.a_col + e);
@@ -201,7 +215,9 @@ __global__ __launch_bounds__(kSampleWarps * kWarp) void k_esc_sample(ProductArgs
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) nip += __shfl_xor_sync(0xffffffffu, nip, o);
-    if (nip == 0 || nip > cap || nip > 3 * kSampleSlots / 4) return;
+    if (nip == 0) return;
+    count_nip(nip, nip > cap);
+    if (nip > cap || nip > 3 * kSampleSlots / 4) return;
     int b = 0;
     while (nip > lim.limit[b]) b++;
     int32_t* tab = s_tab[wid];

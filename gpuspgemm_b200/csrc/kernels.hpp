@@ -101,7 +101,7 @@ int s2n_esc_ladder_f32(const BinLauncher** out);
 // Sampled compression of the first kEscBins fill bins of a one-pass product:
 // the NIP and exact nnz of up to `samples` rows spread evenly over A, summed
 // per team bin (rows binned by NIP with `lim`; rows above the last limit are
-// skipped).  `p` needs A, B and the status word.
+// only counted in nip_above).  `p` needs A, B and the status word.
 constexpr int kEscBins = 4;
 constexpr int kEscSamples = 4096;
 // A team bin expands, sorts and compresses when its sampled NIP / nnz is at
@@ -109,12 +109,22 @@ constexpr int kEscSamples = 4096;
 // crossovers: none up to NIP/nnz 4 for rows of <= 48 products, ~1.45 at
 // <= 192, ~1.1 at <= 768).
 constexpr double kEscMaxRatio[kEscBins] = {8.0, 8.0, 1.4, 1.1};
+// The sample runs for products with at least this many entries in A.
+constexpr int64_t kSampleMinNnz = int64_t(1) << 16;
+// Auto mode keeps two passes when at least this share of the sampled NIP
+// lies in rows above the team bins (one pass bins them by NIP into the CTA
+// bins, two passes by nnz into small team tables) and the team bins' sampled
+// NIP / nnz is at least kTwoPassMinRatio.
+constexpr double kTwoPassMinShare = 0.5;
+constexpr double kTwoPassMinRatio = 4.0;
 struct EscLimits {
     int32_t limit[kEscBins];
 };
 struct EscSample {
     int64_t nip[kEscBins];
     int64_t nnz[kEscBins];
+    int64_t nip_seen;   // NIP of every sampled row (A-row length for rows
+    int64_t nip_above;  // longer than the last limit), and of those above it
 };
 cudaError_t launch_esc_sample(const ProductArgs& p, int32_t m, int32_t samples,
                               const EscLimits& lim, EscSample* out, cudaStream_t s);

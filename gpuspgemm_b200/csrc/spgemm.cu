@@ -99,6 +99,12 @@ struct spgemm_handle_s {
     size_t scratch_bytes = 0;
     uint32_t* bitmaps = nullptr;
     size_t bitmap_bytes = 0;
+    // one-pass temporaries (NIP slots, their columns and values): grown,
+    // never shrunk, like the scratch.  Taking them from the pool per call
+    // cost ~2.7 ms of host time whenever live results had fragmented it
+    // (products of different shapes in turn, as in R * (A * P)).
+    void* onepass = nullptr;
+    size_t onepass_bytes = 0;
     b200::HostMirror* mirror = nullptr;  // pinned
     // host-operand staging on the device
     void* in_buf = nullptr;
@@ -425,6 +431,7 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     C->rpt = c_rpt;
     auto bail = [&](spgemm_status st) {
         const std::string msg = g_last_error;
+        cudaStreamSynchronize(h->side[0]);  // a compression sample may still read A and B
         cudaStreamSynchronize(stream);
         spgemm_csr_free(C, stream);
         cudaStreamSynchronize(stream);
@@ -513,6 +520,10 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     // kernels, the scan binning and their second pass over every product with
     // one copy of C, at the price of temporaries of NIP entries.  Plans keep
     // the two-pass path (their graph replays the fill alone).
+    //
+    // In auto mode a compression sample taken beside the fill binning can
+    // still send the product to two passes (rows above the team bins that
+    // repeat many columns); the binning by NIP is then the only work lost.
     const int64_t nip_total = p1.total_key;
     const bool one_pass =
         cr == nullptr && h->one_pass != 2 && nip_total <= INT32_MAX &&
@@ -524,13 +535,7 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         int32_t* off = nullptr;
         int32_t* tmp_col = nullptr;
         void* tmp_val = nullptr;
-        bool sampling = false;  // the compression sample may still read A and B
-        auto release = [&]() {
-            if (sampling) cudaStreamWaitEvent(stream, h->ev_sample, 0);
-            if (off) cudaFreeAsync(off, stream);
-            if (tmp_col) cudaFreeAsync(tmp_col, stream);
-            if (tmp_val) cudaFreeAsync(tmp_val, stream);
-        };
+        auto release = [&]() {};
 #define B200_ONE(expr)                                                   \
     do {                                                                 \
         spgemm_status st_ = (expr);                                      \
@@ -548,9 +553,18 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         }                                                                \
     } while (0)
         // NIP slots: the scan of the NIP per row (c_rpt holds it) into off
-        B200_ONE_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&off),
-                                              sizeof(int32_t) * (size_t(m) + 1), h->pool, stream),
-                      "allocate NIP slots");
+        {
+            // off (m + 1 slot starts), tmp_col (NIP + 4 columns: a row's tail
+            // never leaves the buffer), tmp_val (NIP values), 256-byte aligned
+            const size_t o_col = align_up(sizeof(int32_t) * (size_t(m) + 1), 256);
+            const size_t o_val = align_up(o_col + sizeof(int32_t) * size_t(nip_total) + 16, 256);
+            const size_t need = o_val + sizeof(V) * size_t(nip_total);
+            B200_ONE(regrow(h, &h->onepass, &h->onepass_bytes, need, stream));
+            char* base = static_cast<char*>(h->onepass);
+            off = reinterpret_cast<int32_t*>(base);
+            tmp_col = reinterpret_cast<int32_t*>(base + o_col);
+            tmp_val = base + o_val;
+        }
         B200_ONE_CUDA(cudaMemcpyAsync(off, c_rpt, sizeof(int32_t) * size_t(m),
                                       cudaMemcpyDeviceToDevice, stream),
                       "copy NIP per row");
@@ -559,9 +573,10 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         BinLauncher one_fil[16];
         for (int b = 0; b < nfil && b < 16; b++) one_fil[b] = fil[b];
         const bool esc_ok = narrow && h->esc != 2;
-        const bool esc_sampled = esc_ok && h->esc == 0;
+        const bool esc_sampled = esc_ok && h->esc == 0;  // by the sample, if it ran
         const Ladder ladf = make_ladder(fil, nfil, h->min_num_bin);
-        if (esc_sampled) {
+        const bool sampled = (h->one_pass == 0 || esc_sampled) && A->nnz >= kSampleMinNnz;
+        if (sampled) {
             // the compression sample reads A and B only: it runs on a side
             // stream beside the fill binning and joins before the host sync
             EscLimits el{};
@@ -572,13 +587,10 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
                           "reset the compression sample");
             B200_ONE_CUDA(cudaEventRecord(h->ev_fork, stream), "fork the sample stream");
             B200_ONE_CUDA(cudaStreamWaitEvent(side, h->ev_fork, 0), "fork the sample stream");
-            const spgemm_status st_sample =
-                timed(h, "esc_sample", 2, -1, samples, side,
-                      [&](cudaStream_t ss) { return launch_esc_sample(pa, m, samples, el, s.sample, ss); });
-            // recorded whatever the launch returned, so an error path can wait on it
+            B200_ONE(timed(h, "esc_sample", 2, -1, samples, side, [&](cudaStream_t ss) {
+                return launch_esc_sample(pa, m, samples, el, s.sample, ss);
+            }));
             B200_ONE_CUDA(cudaEventRecord(h->ev_sample, side), "join the sample stream");
-            sampling = true;
-            B200_ONE(st_sample);
         }
         B200_ONE(timed(h, "nip_fill_hist", 2, -1, m, stream, [&](cudaStream_t ss) {
             return launch_nnz_hist(off, m, s.hist2, s.cta_sum, s.plan2, ladf, ss);
@@ -590,31 +602,40 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
             return launch_bin_scatter(off, m, s.hist2, s.cta_sum, s.bins2, s.plan2, ladf, true,
                                       ss);
         }));
-        // C.rpt receives each row's exact nnz (rows without products stay 0)
-        B200_ONE_CUDA(cudaMemsetAsync(c_rpt, 0, sizeof(int32_t) * (size_t(m) + 1), stream),
-                      "memset row counts");
-        B200_ONE_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&tmp_col),
-                                              sizeof(int32_t) * size_t(nip_total) + 16, h->pool,
-                                              stream),
-                      "allocate the one-pass columns");
-        B200_ONE_CUDA(cudaMallocFromPoolAsync(&tmp_val, sizeof(V) * size_t(nip_total), h->pool,
-                                              stream),
-                      "allocate the one-pass values");
         mark(2);
-        if (esc_sampled) {
+        if (sampled)
             B200_ONE_CUDA(cudaStreamWaitEvent(stream, h->ev_sample, 0), "join the sample stream");
-            sampling = false;
-        }
-        B200_ONE(sync_mirror(h, stream, s.plan2, s, esc_sampled));
+        B200_ONE(sync_mirror(h, stream, s.plan2, s, sampled));
         mark(3);
         B200_ONE(status_to_error(h->mirror->status));
         const Plan pf = h->mirror->plan;
+        const EscSample es = h->mirror->sample;
+        // sampled: the NIP of rows above the team bins, the team bins' NIP/nnz
+        int64_t team_nip = 0;
+        int64_t team_nnz = 0;
+        for (int b = 0; b < kEscBins; b++) {
+            team_nip += es.nip[b];
+            team_nnz += es.nnz[b];
+        }
+        const bool wide_rows_compress =
+            sampled && es.nip_seen > 0 && team_nnz > 0 &&
+            static_cast<double>(es.nip_above) >=
+                kTwoPassMinShare * static_cast<double>(es.nip_seen) &&
+            static_cast<double>(team_nip) >= kTwoPassMinRatio * static_cast<double>(team_nnz);
+        if (h->one_pass == 0 && wide_rows_compress) {
+            // two passes after all: C.rpt still holds the NIP per row; the
+            // fill binning's plan is reused by the scan pass
+            h->info.one_pass = 0;
+            B200_ONE_CUDA(cudaMemsetAsync(s.plan2, 0, sizeof(Plan), stream), "reset a plan");
+        } else {
+        // C.rpt receives each row's exact nnz (rows without products stay 0)
+        B200_ONE_CUDA(cudaMemsetAsync(c_rpt, 0, sizeof(int32_t) * (size_t(m) + 1), stream),
+                      "memset row counts");
         if (esc_ok) {
             const BinLauncher* esc = nullptr;
             const int nesc = sizeof(V) == 8 ? s2n_esc_ladder_f64(&esc) : s2n_esc_ladder_f32(&esc);
-            const EscSample& es = h->mirror->sample;
             for (int b = 0; b < kEscBins && b < nesc && b < nfil; b++) {
-                const bool use = !esc_sampled || (es.nnz[b] > 0 &&
+                const bool use = !esc_sampled || (sampled && es.nnz[b] > 0 &&
                                                   static_cast<double>(es.nip[b]) <=
                                                       kEscMaxRatio[b] * static_cast<double>(es.nnz[b]));
                 if (use) {
@@ -684,9 +705,10 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         mark(6);
         h->info.host_syncs++;
         resolve_profile(h);
+        return SPGEMM_OK;
+        }
 #undef B200_ONE_CUDA
 #undef B200_ONE
-        return SPGEMM_OK;
     }
 
     // ---- sym1: exact nnz per row --------------------------------------------
@@ -1702,6 +1724,7 @@ spgemm_status spgemm_destroy(spgemm_handle_t h) {
     if (h->ev_sample) cudaEventDestroy(h->ev_sample);
     if (h->scratch) cudaFree(h->scratch);
     if (h->bitmaps) cudaFree(h->bitmaps);
+    if (h->onepass) cudaFree(h->onepass);
     if (h->in_buf) cudaFree(h->in_buf);
     if (h->mirror) cudaFreeHost(h->mirror);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);

@@ -184,19 +184,25 @@ typedef enum spgemm_option {
      * of its row-sort ladder (-1 = off). */
     SPGEMM_OPT_MIN_TRANSPOSE_BIN = 7,
     /* How the row sizes of C are found.  0 (default): one pass when the
-     * product has at least 2^21 intermediate products (NIP) and its
-     * temporaries -- NIP entries of column and value -- fit 4 GiB, else two;
-     * 1: always one pass; 2: always two passes.  Two passes: the hash count
-     * kernels give each row's exact nnz, the fill writes C in place.  One
-     * pass: rows are filled into NIP-sized slots while their nnz is counted,
-     * then compacted into C -- no count kernels, one more copy of C. */
+     * product has at least 2^21 intermediate products (NIP), its
+     * temporaries -- NIP entries of column and value -- fit 4 GiB, and a
+     * sample of 4,096 rows of A (products with A.nnz >= 2^16) does not show
+     * most of the NIP in rows of more than 768 products whose columns repeat
+     * on average 4 times or more (those fill far smaller tables in two
+     * passes); else two.  1: always one pass; 2: always two passes.  Two
+     * passes: the hash count kernels give each row's exact nnz, the fill
+     * writes C in place.  One pass: rows are filled into NIP-sized slots
+     * while their nnz is counted, then compacted into C -- no count kernels,
+     * one more copy of C.  The one-pass temporaries belong to the handle and
+     * are kept for its next products (freed with the handle). */
     SPGEMM_OPT_ONE_PASS = 8,
     /* One-pass products with B.n <= 2^20: whether the four team fill bins
      * (rows of up to 12, 48, 192 and 768 intermediate products) expand, sort
      * and compress -- stage every product, sort by column, sum each column's
      * run in product order -- instead of hashing.  0 (default): per bin,
-     * when the NIP / nnz of up to 64 sampled rows of the bin is at most 1.5;
-     * 1: always; 2: never.  spgemm_info.esc_mask says which bins did. */
+     * when the NIP / nnz of the bin's rows among 4,096 rows sampled from A is
+     * at most 8, 8, 1.4 and 1.1 (products with A.nnz >= 2^16; smaller ones
+     * hash); 1: always; 2: never.  spgemm_info.esc_mask says which bins did. */
     SPGEMM_OPT_ESC = 9
 } spgemm_option;
 

@@ -313,6 +313,30 @@ def test_bitmap_bin_back_to_back(handle, oracle_mod, passes):
         handle.set_option(N.OPT_ONE_PASS, 0)
 
 
+def test_compressing_wide_rows_keep_two_passes(handle, oracle_mod):
+    """By default a product whose NIP lies mostly in rows above the team
+    bins (> 768 products) that repeat their columns many times -- R * (A * P)
+    of a 27-point stencil on 50^3, NIP/nnz 33 -- keeps two passes: in one pass
+    those rows would fill NIP-sized CTA tables, in two passes nnz-sized team
+    tables.  Both modes give the same C."""
+    from gpuspgemm_b200 import _native as N
+    A = G.stencil27(50)
+    P = G.aggregation_prolongator(50, seed=3)
+    R = oracle_mod.transpose(P)
+    AP = oracle_mod.spgemm(A, P)
+    assert oracle_mod.nip(R, AP) >= 1 << 21 and R.nnz >= 1 << 16
+    C2 = gpu_product(R, AP, handle, np.float64)
+    assert handle.info()["one_pass"] == 0
+    handle.set_option(N.OPT_ONE_PASS, 1)
+    try:
+        C1 = gpu_product(R, AP, handle, np.float64)
+        assert handle.info()["one_pass"] == 1
+    finally:
+        handle.set_option(N.OPT_ONE_PASS, 0)
+    assert np.array_equal(C1.rpt, C2.rpt) and np.array_equal(C1.col, C2.col)
+    check(oracle_mod, R, AP, C2, np.float64, "rap50_two_pass")
+
+
 def test_one_pass_chosen_and_equal_to_two_pass(handle, oracle_mod):
     """By default a product whose temporaries fit runs one pass; its C equals
     the two-pass C in structure, and both match the oracle."""
