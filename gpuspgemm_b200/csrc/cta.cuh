@@ -66,13 +66,16 @@ __device__ __forceinline__ int block_sum(int v, int32_t* warp_tot) {
 // Walk the intermediate products of the A-row segment [a0, a1) with the whole
 // CTA.  Chunks of THREADS A entries are scanned once; then every thread takes
 // products q = tid, tid + THREADS, ... of the chunk and finds its A entry by a
-// binary search of the chunk's prefix.  Calls f(q_b, a_index).  All threads
-// must call it (it contains barriers).
+// binary search of the chunk's prefix.  Calls f(q_b, a_index, q_row) with
+// q_row the product's place in the row's flattened sequence (products of A
+// entry a0 first, each B row in order).  All threads must call it (it
+// contains barriers).
 template<int THREADS, typename F>
-__device__ __forceinline__ void cta_for_products(const int32_t* __restrict__ a_col,
-                                                 const int32_t* __restrict__ b_rpt, int a0,
-                                                 int a1, CtaScratch<THREADS>& sc, F&& f) {
+__device__ __forceinline__ void cta_for_products_at(const int32_t* __restrict__ a_col,
+                                                    const int32_t* __restrict__ b_rpt, int a0,
+                                                    int a1, CtaScratch<THREADS>& sc, F&& f) {
     const int tid = threadIdx.x;
+    int off = 0;  // products of the chunks before this one
     for (int base = a0; base < a1; base += THREADS) {
         const int e = base + tid;
         int bs = 0;
@@ -97,10 +100,20 @@ __device__ __forceinline__ void cta_for_products(const int32_t* __restrict__ a_c
                 lo = (sc.exc[lo + half] <= q) ? lo + half : lo;
                 n -= half;
             }
-            f(sc.bs[lo] + q - sc.exc[lo], base + lo);
+            f(sc.bs[lo] + q - sc.exc[lo], base + lo, off + q);
         }
+        off += total;
         __syncthreads();
     }
+}
+
+// The same walk for callers that need no product position: f(q_b, a_index).
+template<int THREADS, typename F>
+__device__ __forceinline__ void cta_for_products(const int32_t* __restrict__ a_col,
+                                                 const int32_t* __restrict__ b_rpt, int a0,
+                                                 int a1, CtaScratch<THREADS>& sc, F&& f) {
+    cta_for_products_at<THREADS>(a_col, b_rpt, a0, a1, sc,
+                                 [&](int qb, int ai, int) { f(qb, ai); });
 }
 
 // Column window of one row of C: the smallest first column and the largest

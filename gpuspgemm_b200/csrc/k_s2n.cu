@@ -169,6 +169,97 @@ __global__ __launch_bounds__(THREADS) void k_esc_team(ProductArgs p) {
     if (lane == 0) p.row_nnz[row] = written;
 }
 
+// Expand-sort-compress for rows of up to NMAX products with a whole CTA (the
+// 256-thread bin's range).  As the team version, with an unsigned key
+// (column << SHIFT | q), SHIFT = log2 of the sort capacity, stored with its
+// top bit flipped so that the signed register sort orders it as unsigned
+// (B.n <= 2^(32 - SHIFT)).  Compression: each thread takes a contiguous run
+// of sorted positions, counts the column heads in it, a block scan gives its
+// first output slot, and each head sums its column's run (which may run into
+// the next thread's positions) in product order.
+template<typename V, int THREADS, int NMAX>
+struct EscCtaLayout {
+    static constexpr int P = next_pow2(NMAX);
+    static constexpr int K = P > THREADS * 16 ? P : THREADS * 16;  // sort slots
+    static constexpr int SHIFT = ilog2(P);
+    static constexpr size_t vals_bytes = sizeof(V) * NMAX;
+    static constexpr size_t keys_bytes = sizeof(int32_t) * K;
+    static constexpr size_t bytes = vals_bytes + keys_bytes + sizeof(CtaScratch<THREADS>);
+    static_assert(NMAX <= THREADS * 16, "the register sort takes THREADS * 16 keys");
+    static_assert(bytes <= 232448, "an ESC CTA bin's shared memory exceeds 227 KB");
+};
+
+template<typename V, int THREADS, int NMAX>
+__global__ __launch_bounds__(THREADS) void k_esc_cta(ProductArgs p) {
+    using L = EscCtaLayout<V, THREADS, NMAX>;
+    constexpr int SHIFT = L::SHIFT;
+    constexpr uint32_t QMASK = (1u << SHIFT) - 1u;
+    constexpr int NW = THREADS / kWarp;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* vals = reinterpret_cast<V*>(smem_raw);
+    int32_t* keys = reinterpret_cast<int32_t*>(smem_raw + L::vals_bytes);
+    auto& sc = *reinterpret_cast<CtaScratch<THREADS>*>(smem_raw + L::vals_bytes + L::keys_bytes);
+    const int tid = threadIdx.x;
+    const int row = p.rows[blockIdx.x];
+    const int c0 = p.c_rpt[row];
+    const int nip = p.c_rpt[row + 1] - c0;  // the row's NIP-sized slot
+    if (nip > NMAX || p.row_nnz == nullptr) {
+        if (tid == 0) report(p.status, kStCapacity, row, nip);
+        return;
+    }
+    cta_for_products_at<THREADS>(p.a_col, p.b_rpt, p.a_rpt[row], p.a_rpt[row + 1], sc,
+                                 [&](int qb, int ai, int q) {
+                                     if (q >= NMAX) return;
+                                     int32_t col = __ldg(p.b_col + qb);
+                                     if (static_cast<uint32_t>(col) >=
+                                         static_cast<uint32_t>(p.n_cols)) {
+                                         report(p.status, kStBadInput, row, col);
+                                         col = 0;
+                                     }
+                                     const uint32_t u =
+                                         (static_cast<uint32_t>(col) << SHIFT) | static_cast<uint32_t>(q);
+                                     keys[q] = static_cast<int32_t>(u ^ 0x80000000u);
+                                     vals[q] = ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb);
+                                 });
+    cta_sort_swz<THREADS>(keys, nip);
+    auto unkey = [&](int i) { return static_cast<uint32_t>(keys[swz(i)]) ^ 0x80000000u; };
+    const int per = (nip + THREADS - 1) / THREADS;
+    const int i0 = min(tid * per, nip);
+    const int i1 = min(i0 + per, nip);
+    int heads = 0;
+    {
+        uint32_t prev = i0 > 0 ? (unkey(i0 - 1) >> SHIFT) : 0xffffffffu;
+        for (int i = i0; i < i1; i++) {
+            const uint32_t c = unkey(i) >> SHIFT;
+            heads += c != prev;
+            prev = c;
+        }
+    }
+    const int inc = block_inclusive_scan<THREADS>(heads, sc.warp_tot);
+    const int total = sc.warp_tot[NW - 1];
+    int r = inc - heads;
+    int32_t* out_col = p.c_col + c0;
+    V* out_val = static_cast<V*>(p.c_val) + c0;
+    uint32_t prev = i0 > 0 ? (unkey(i0 - 1) >> SHIFT) : 0xffffffffu;
+    for (int i = i0; i < i1; i++) {
+        const uint32_t u = unkey(i);
+        const uint32_t c = u >> SHIFT;
+        if (c != prev) {
+            V sum = vals[u & QMASK];
+            for (int k = i + 1; k < nip; k++) {
+                const uint32_t w = unkey(k);
+                if ((w >> SHIFT) != c) break;
+                sum += vals[w & QMASK];
+            }
+            out_col[r] = static_cast<int32_t>(c);
+            out_val[r] = sum;
+            r++;
+        }
+        prev = c;
+    }
+    if (tid == 0) p.row_nnz[row] = total;
+}
+
 // Compression of the team bins, sampled: `samples` rows spread evenly over
 // A are counted exactly (one warp per row, a 1024-slot shared hash set) when
 // their NIP is at most the last team bin's limit, and their NIP and nnz are
@@ -514,6 +605,12 @@ cudaError_t launch_esc(const ProductArgs& p, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template<typename V, int THREADS, int NMAX>
+cudaError_t launch_esc_cta(const ProductArgs& p, cudaStream_t s) {
+    k_esc_cta<V, THREADS, NMAX><<<p.nrows, THREADS, EscCtaLayout<V, THREADS, NMAX>::bytes, s>>>(p);
+    return cudaGetLastError();
+}
+
 template<typename V, int THREADS, int T, int CAP>
 cudaError_t launch_cta(const ProductArgs& p, cudaStream_t s) {
     k_s2n_cta<V, THREADS, T, CAP>
@@ -596,9 +693,9 @@ B200_S2N_BITMAP_LADDER(double)
 B200_S2N_BITMAP_LADDER(float)
 #undef B200_S2N_BITMAP_LADDER
 
-// One-pass ladder for B.n <= kBitmapCols: the team bins expand, sort and
-// compress (k_esc_team) with the hash team bins' row limits; the rest is the
-// bitmap ladder.
+// One-pass ladder for B.n <= kBitmapCols: the team bins and the 256-thread
+// bin expand, sort and compress (k_esc_team, k_esc_cta) with the hash bins'
+// row limits; the bitmap and global bins are the bitmap ladder's.
 template<typename V>
 struct S2nEscLadder {
     static const BinLauncher entries[];
@@ -616,8 +713,9 @@ struct S2nEscLadder {
          launch_esc<V, 16, 256, 192>},                                                        \
         {BinKind::Team, 768, 8, 256, EscLayout<V, 32, 256, 768>::bytes, "esc_team32_n768",    \
          launch_esc<V, 32, 256, 768>},                                                        \
-        S2nBitmapLadder<V>::entries[4], S2nBitmapLadder<V>::entries[5],                       \
-        S2nBitmapLadder<V>::entries[6],                                                       \
+        {BinKind::Cta, 3072, 1, 256, EscCtaLayout<V, 256, 3072>::bytes, "esc_cta256_n3072",    \
+         launch_esc_cta<V, 256, 3072>},                                                       \
+        S2nBitmapLadder<V>::entries[5], S2nBitmapLadder<V>::entries[6],                       \
     };                                                                                        \
     template<>                                                                                \
     const int S2nEscLadder<V>::count = sizeof(S2nEscLadder<V>::entries) / sizeof(BinLauncher);
@@ -645,6 +743,7 @@ cudaError_t prepare_one() {
     B200_SMEM((k_esc_team<V, 8, 256, 48>), (EscLayout<V, 8, 256, 48>::bytes));
     B200_SMEM((k_esc_team<V, 16, 256, 192>), (EscLayout<V, 16, 256, 192>::bytes));
     B200_SMEM((k_esc_team<V, 32, 256, 768>), (EscLayout<V, 32, 256, 768>::bytes));
+    B200_SMEM((k_esc_cta<V, 256, 3072>), (EscCtaLayout<V, 256, 3072>::bytes));
 #undef B200_SMEM
     return e;
 }

@@ -93,8 +93,8 @@ constexpr int kBitmapCols = 1 << 20;
 int s2n_bitmap_ladder_f64(const BinLauncher** out);
 int s2n_bitmap_ladder_f32(const BinLauncher** out);
 // One-pass ladder for B.n <= kBitmapCols (key = NIP of the row): the team bins
-// expand, sort and compress; then the bitmap ladder's CTA, bitmap and global
-// bins.  Same bin count and limits as the bitmap ladder.
+// and the 256-thread bin expand, sort and compress; then the bitmap ladder's
+// bitmap and global bins.  Same bin count and limits as the bitmap ladder.
 int s2n_esc_ladder_f64(const BinLauncher** out);
 int s2n_esc_ladder_f32(const BinLauncher** out);
 
@@ -109,6 +109,9 @@ constexpr int kEscSamples = 4096;
 // crossovers: none up to NIP/nnz 4 for rows of <= 48 products, ~1.45 at
 // <= 192, ~1.1 at <= 768).
 constexpr double kEscMaxRatio[kEscBins] = {8.0, 8.0, 1.4, 1.1};
+// The one-pass ladder's bins that may expand-sort-compress: the team bins and
+// the 256-thread bin, which follows the sample of the largest team bin.
+constexpr int kEscLadderBins = kEscBins + 1;
 // The sample runs for products with at least this many entries in A.
 constexpr int64_t kSampleMinNnz = int64_t(1) << 16;
 // Auto mode keeps two passes when at least this share of the sampled NIP

@@ -634,10 +634,11 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         if (esc_ok) {
             const BinLauncher* esc = nullptr;
             const int nesc = sizeof(V) == 8 ? s2n_esc_ladder_f64(&esc) : s2n_esc_ladder_f32(&esc);
-            for (int b = 0; b < kEscBins && b < nesc && b < nfil; b++) {
-                const bool use = !esc_sampled || (sampled && es.nnz[b] > 0 &&
-                                                  static_cast<double>(es.nip[b]) <=
-                                                      kEscMaxRatio[b] * static_cast<double>(es.nnz[b]));
+            for (int b = 0; b < kEscLadderBins && b < nesc && b < nfil; b++) {
+                const int sb = b < kEscBins ? b : kEscBins - 1;  // the CTA bin: the last team bin's sample
+                const bool use = !esc_sampled || (sampled && es.nnz[sb] > 0 &&
+                                                  static_cast<double>(es.nip[sb]) <=
+                                                      kEscMaxRatio[sb] * static_cast<double>(es.nnz[sb]));
                 if (use) {
                     one_fil[b] = esc[b];
                     h->info.esc_mask |= 1 << b;

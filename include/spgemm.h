@@ -100,7 +100,7 @@ typedef struct spgemm_info {
      * fill kernels queued, final sync done (unused entries 0) */
     float phase_us[8];
     int32_t one_pass;        /* 1: C's row sizes came from the one-pass fill */
-    int32_t esc_mask;        /* bit b: one-pass team bin b expanded, sorted and compressed */
+    int32_t esc_mask;        /* bit b: one-pass fill bin b expanded, sorted and compressed */
 } spgemm_info;
 
 /* ---- lifecycle ------------------------------------------------------------ */
@@ -197,12 +197,14 @@ typedef enum spgemm_option {
      * are kept for its next products (freed with the handle). */
     SPGEMM_OPT_ONE_PASS = 8,
     /* One-pass products with B.n <= 2^20: whether the four team fill bins
-     * (rows of up to 12, 48, 192 and 768 intermediate products) expand, sort
-     * and compress -- stage every product, sort by column, sum each column's
-     * run in product order -- instead of hashing.  0 (default): per bin,
-     * when the NIP / nnz of the bin's rows among 4,096 rows sampled from A is
-     * at most 8, 8, 1.4 and 1.1 (products with A.nnz >= 2^16; smaller ones
-     * hash); 1: always; 2: never.  spgemm_info.esc_mask says which bins did. */
+     * (rows of up to 12, 48, 192 and 768 intermediate products) and the
+     * 256-thread bin (up to 3,072) expand, sort and compress -- stage every
+     * product, sort by column, sum each column's run in product order --
+     * instead of hashing.  0 (default): per bin, when the NIP / nnz of the
+     * bin's rows among 4,096 rows sampled from A is at most 8, 8, 1.4 and 1.1
+     * (the 256-thread bin follows the last team bin's sample; products with
+     * A.nnz >= 2^16 -- smaller ones hash); 1: always; 2: never.
+     * spgemm_info.esc_mask says which bins did (bits 0-4). */
     SPGEMM_OPT_ESC = 9
 } spgemm_option;
 

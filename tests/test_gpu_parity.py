@@ -243,7 +243,7 @@ def test_one_pass_esc_bins(handle, oracle_mod, esc, dtype):
             C = gpu_product(A, B, handle, dtype)
             info = handle.info()
             assert info["one_pass"] == 1
-            assert info["esc_mask"] == {1: 0b1111, 2: 0}.get(esc, info["esc_mask"])
+            assert info["esc_mask"] == {1: 0b11111, 2: 0}.get(esc, info["esc_mask"])
             check(oracle_mod, A, B, C, dtype, f"esc{esc}_{name}")
     finally:
         handle.set_option(N.OPT_ONE_PASS, 0)
@@ -251,15 +251,16 @@ def test_one_pass_esc_bins(handle, oracle_mod, esc, dtype):
 
 
 def test_esc_chosen_by_sampled_compression(handle, oracle_mod):
-    """By default a team bin expands, sorts and compresses only when its
-    sampled rows repeat few columns: every team bin of a power-law square
-    (NIP/nnz 1.0), none of a 27-point stencil's square (NIP/nnz 4.6-6.0)."""
+    """By default a fill bin expands, sorts and compresses only when its
+    sampled rows repeat few columns: every team bin and the 256-thread bin of
+    a power-law square (NIP/nnz 1.0), none of a 27-point stencil's square
+    (NIP/nnz 4.6-6.0)."""
     from gpuspgemm_b200 import _native as N
     handle.set_option(N.OPT_ONE_PASS, 1)
     try:
         P = G.power_law(30000, 2.0, 3000, seed=21)
         C = gpu_product(P, P, handle, np.float64)
-        assert handle.info()["esc_mask"] == 0b1111
+        assert handle.info()["esc_mask"] == 0b11111
         check(oracle_mod, P, P, C, np.float64, "esc_auto_power_law", positive=True)
         S = G.stencil27(12)
         C = gpu_product(S, S, handle, np.float64)
@@ -271,9 +272,10 @@ def test_esc_chosen_by_sampled_compression(handle, oracle_mod):
 
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 def test_esc_sums_in_oracle_order(handle, oracle_mod, dtype):
-    """Rows of at most 768 products all expand, sort and compress, which sums
-    each entry of C over its products in the oracle's (Gustavson) order with
-    the same roundings: the values are bit-exact, not just within tolerance."""
+    """Rows of at most 3,072 products all expand, sort and compress (team
+    bins and the 256-thread bin), which sums each entry of C over its products
+    in the oracle's (Gustavson) order with the same roundings: the values are
+    bit-exact, not just within tolerance."""
     from gpuspgemm_b200 import _native as N
     dtype = np.dtype(dtype)
     handle.set_option(N.OPT_ONE_PASS, 1)
@@ -281,9 +283,10 @@ def test_esc_sums_in_oracle_order(handle, oracle_mod, dtype):
     try:
         for A, B in [(G.stencil27(12), G.stencil27(12)),  # NIP up to 729 per row
                      (G.uniform_rows(4096, 8), G.uniform_rows(4096, 8)),
-                     (G.power_law(3000, 2.0, 40, seed=7), G.power_law(3000, 2.0, 40, seed=7))]:
+                     (G.power_law(3000, 2.0, 40, seed=7), G.power_law(3000, 2.0, 40, seed=7)),
+                     (G.power_law(3000, 2.0, 300, seed=42), G.power_law(3000, 2.0, 300, seed=42))]:
             A, B = A.astype(dtype), B.astype(dtype)
-            assert oracle_mod.nip(A, B, per_row=True)[1].max() <= 768
+            assert oracle_mod.nip(A, B, per_row=True)[1].max() <= 3072
             C = gpu_product(A, B, handle, dtype)
             R = oracle_mod.spgemm(A, B, dtype)
             assert np.array_equal(C.rpt, R.rpt) and np.array_equal(C.col, R.col)
