@@ -132,7 +132,10 @@ __global__ __launch_bounds__(kBinThreads) void k_nip_hist(
 // ---- pass 1': nnz histogram + per-CTA nnz sums ----------------------------
 __global__ __launch_bounds__(kBinThreads) void k_nnz_hist(
     const int32_t* __restrict__ c_rpt, int32_t m, int32_t* __restrict__ hist,
-    int64_t* __restrict__ cta_sum, Plan* __restrict__ plan, const __grid_constant__ Ladder lad) {
+    int64_t* __restrict__ cta_sum, Plan* __restrict__ plan, const __grid_constant__ Ladder lad,
+    const Ladder* __restrict__ dlad) {
+    // limits chosen on the device (nullptr: the launch's own)
+    const Ladder& L = dlad != nullptr ? *dlad : lad;
     __shared__ int32_t s_hist[kMaxBins];
     __shared__ long long s_tot[kBinThreads / kWarp];
     __shared__ int32_t s_max[kBinThreads / kWarp];
@@ -149,7 +152,7 @@ __global__ __launch_bounds__(kBinThreads) void k_nnz_hist(
             const int32_t key = c_rpt[r];
             my_tot += key;
             my_max = max(my_max, key);
-            if (key > 0) atomicAdd(&s_hist[find_bin(lad, key)], 1);
+            if (key > 0) atomicAdd(&s_hist[find_bin(L, key)], 1);
         }
     }
     my_tot = warp_sum_ll(my_tot);
@@ -234,7 +237,9 @@ __global__ __launch_bounds__(kOffThreads) void k_bin_offsets(int32_t* __restrict
 __global__ __launch_bounds__(kBinThreads) void k_bin_scatter(
     int32_t* __restrict__ c_rpt, int32_t m, const int32_t* __restrict__ hist_off,
     const int64_t* __restrict__ cta_off, int32_t* __restrict__ bins,
-    const Plan* __restrict__ plan, const __grid_constant__ Ladder lad, int scan) {
+    const Plan* __restrict__ plan, const __grid_constant__ Ladder lad, int scan,
+    const Ladder* __restrict__ dlad) {
+    const Ladder& L = dlad != nullptr ? *dlad : lad;  // limits chosen on the device, if any
     constexpr int NW = kBinThreads / kWarp;
     __shared__ int32_t s_base[kMaxBins];
     __shared__ int32_t s_off[kMaxBins];
@@ -255,7 +260,7 @@ __global__ __launch_bounds__(kBinThreads) void k_bin_scatter(
     for (int it = 0; it < kBinRowsPerCta / kBinThreads; it++) {
         const int r = blockIdx.x * kBinRowsPerCta + it * kBinThreads + tid;
         const int32_t key = r < m ? c_rpt[r] : 0;
-        const int bin = key > 0 ? find_bin(lad, key) : -1;
+        const int bin = key > 0 ? find_bin(L, key) : -1;
         const unsigned peers = __match_any_sync(0xffffffffu, bin);
         const int lrank = __popc(peers & lt_mask);
         long long x = key;
@@ -426,10 +431,10 @@ cudaError_t launch_nip_hist(const int32_t* a_rpt, const int32_t* a_col, const in
 }
 
 cudaError_t launch_nnz_hist(const int32_t* c_rpt, int32_t m, int32_t* hist, int64_t* cta_sum,
-                            Plan* plan, const Ladder& lad, cudaStream_t s) {
+                            Plan* plan, const Ladder& lad, cudaStream_t s, const Ladder* dlad) {
     const int g = bin_ctas(m);
     if (g == 0) return cudaSuccess;
-    k_nnz_hist<<<g, kBinThreads, 0, s>>>(c_rpt, m, hist, cta_sum, plan, lad);
+    k_nnz_hist<<<g, kBinThreads, 0, s>>>(c_rpt, m, hist, cta_sum, plan, lad, dlad);
     return cudaGetLastError();
 }
 
@@ -441,11 +446,11 @@ cudaError_t launch_bin_offsets(int32_t* hist, int32_t nctas, int64_t* cta_sum, P
 
 cudaError_t launch_bin_scatter(int32_t* c_rpt, int32_t m, const int32_t* hist_off,
                                const int64_t* cta_off, int32_t* bins, const Plan* plan,
-                               const Ladder& lad, bool scan, cudaStream_t s) {
+                               const Ladder& lad, bool scan, cudaStream_t s, const Ladder* dlad) {
     const int g = bin_ctas(m);
     if (g == 0) return cudaSuccess;
     k_bin_scatter<<<g, kBinThreads, 0, s>>>(c_rpt, m, hist_off, cta_off, bins, plan, lad,
-                                            scan ? 1 : 0);
+                                            scan ? 1 : 0, dlad);
     return cudaGetLastError();
 }
 

@@ -788,6 +788,26 @@ cudaError_t launch_esc_sample(const ProductArgs& p, int32_t m, int32_t samples,
     return cudaGetLastError();
 }
 
+__global__ void k_esc_decide(EscSample* sample, const __grid_constant__ Ladder base, int esc_mode,
+                             Ladder* out) {
+    constexpr int b = kEscBins - 1;
+    const int64_t nip = sample->nip[b];
+    const int64_t nnz = sample->nnz[b];
+    const bool split = esc_mode == 1 ||
+                       (esc_mode == 0 && nnz > 0 &&
+                        static_cast<double>(nip) <= kEscMaxRatio[b] * static_cast<double>(nnz));
+    Ladder l = base;
+    if (split) l.limit[b] = kEscSplit;
+    *out = l;
+    sample->split = split ? 1 : 0;
+}
+
+cudaError_t launch_esc_decide(EscSample* sample, const Ladder& base, int esc_mode, Ladder* out,
+                              cudaStream_t s) {
+    k_esc_decide<<<1, 1, 0, s>>>(sample, base, esc_mode, out);
+    return cudaGetLastError();
+}
+
 cudaError_t s2n_prepare() {
     cudaError_t e = prepare_one<double>();
     if (e == cudaSuccess) e = prepare_one<float>();

@@ -128,9 +128,19 @@ struct EscSample {
     int64_t nnz[kEscBins];
     int64_t nip_seen;   // NIP of every sampled row (A-row length for rows
     int64_t nip_above;  // longer than the last limit), and of those above it
+    int32_t split;      // written by launch_esc_decide
+    int32_t pad;
 };
 cudaError_t launch_esc_sample(const ProductArgs& p, int32_t m, int32_t samples,
                               const EscLimits& lim, EscSample* out, cudaStream_t s);
+// The fill binning's limits, decided on the device from the sample: when the
+// largest team bin expands, sorts and compresses (esc_mode 1, or 0 and its
+// sampled NIP/nnz at most kEscMaxRatio), its rows above kEscSplit products
+// go to the 256-thread bin (which then expands, sorts and compresses too):
+// out = base with limit[kEscBins - 1] = kEscSplit, and sample->split = 1.
+constexpr int32_t kEscSplit = 512;
+cudaError_t launch_esc_decide(EscSample* sample, const Ladder& base, int esc_mode, Ladder* out,
+                              cudaStream_t s);
 // One-time per-device attribute setup (dynamic smem opt-in) for all kernels.
 cudaError_t sym1_prepare();
 cudaError_t s2n_prepare();
@@ -147,8 +157,10 @@ cudaError_t launch_nip_hist(const int32_t* a_rpt, const int32_t* a_col, const in
                             int32_t m, int32_t* c_rpt, int32_t* hist, Plan* plan,
                             DevStatus* st, const Ladder& lad, cudaStream_t s);
 // Pass 1' (key = nnz already in c_rpt): per-CTA sums and bin histograms.
+// dlad: limits chosen on the device (same bin count as lad), or nullptr.
 cudaError_t launch_nnz_hist(const int32_t* c_rpt, int32_t m, int32_t* hist, int64_t* cta_sum,
-                            Plan* plan, const Ladder& lad, cudaStream_t s);
+                            Plan* plan, const Ladder& lad, cudaStream_t s,
+                            const Ladder* dlad = nullptr);
 // Pass 2: exclusive offsets of the per-CTA histograms (and of cta_sum when
 // given), bin sizes/offsets into the plan.
 cudaError_t launch_bin_offsets(int32_t* hist, int32_t nctas, int64_t* cta_sum, Plan* plan,
@@ -157,7 +169,8 @@ cudaError_t launch_bin_offsets(int32_t* hist, int32_t nctas, int64_t* cta_sum, P
 // rewrites c_rpt[0..m] as the exclusive scan of the nnz it holds.
 cudaError_t launch_bin_scatter(int32_t* c_rpt, int32_t m, const int32_t* hist_off,
                                const int64_t* cta_off, int32_t* bins, const Plan* plan,
-                               const Ladder& lad, bool scan, cudaStream_t s);
+                               const Ladder& lad, bool scan, cudaStream_t s,
+                               const Ladder* dlad = nullptr);
 // One-pass fill: copy each row's entries from its slot [off[r], ...) of the
 // temporary arrays to [rpt[r], rpt[r+1]) of C (values of value_bytes 4 or 8).
 cudaError_t launch_compact_rows(const int32_t* off, const int32_t* rpt, int32_t m,

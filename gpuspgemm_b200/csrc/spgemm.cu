@@ -63,6 +63,7 @@ struct Scratch {
     int32_t* fail_rows;
     int32_t* fail_count;
     EscSample* sample;
+    Ladder* dladder;  // the one-pass fill binning's limits, decided on the device
 };
 
 struct ProfRec {
@@ -180,6 +181,7 @@ spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s, cudaStre
     const size_t o_plan2 = take(sizeof(Plan));
     const size_t o_fail_count = take(sizeof(int32_t));
     const size_t o_sample = take(sizeof(EscSample));
+    const size_t o_dladder = take(sizeof(Ladder));
     const size_t o_hist1 = take(sizeof(int32_t) * kMaxBins * nctas);
     const size_t o_hist2 = take(sizeof(int32_t) * kMaxBins * nctas);
     const size_t o_sum = take(sizeof(int64_t) * nctas);
@@ -195,6 +197,7 @@ spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s, cudaStre
     s->plan2 = reinterpret_cast<Plan*>(b + o_plan2);
     s->fail_count = reinterpret_cast<int32_t*>(b + o_fail_count);
     s->sample = reinterpret_cast<EscSample*>(b + o_sample);
+    s->dladder = reinterpret_cast<Ladder*>(b + o_dladder);
     s->hist1 = reinterpret_cast<int32_t*>(b + o_hist1);
     s->hist2 = reinterpret_cast<int32_t*>(b + o_hist2);
     s->cta_sum = reinterpret_cast<int64_t*>(b + o_sum);
@@ -481,6 +484,43 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         return launch_nip_hist(A->rpt, A->col, B->rpt, m, c_rpt, s.hist1, s.plan1, s.status,
                                lad1, ss);
     }));
+    // Compression sample (products that may run one pass): it reads A and B
+    // only and runs on a side stream after the NIP pass, beside the NIP
+    // binning and the host's first synchronisation, then decides the one-pass
+    // fill binning's limits on the device.  Its sums come back with the fill
+    // binning's plan: they choose one pass or two and, per fill bin,
+    // expand-sort-compress or hashing.
+    const Ladder ladf = make_ladder(fil, nfil, h->min_num_bin);
+    const int esc_mode = (narrow && h->esc != 2) ? h->esc : 2;
+    const bool sampled = cr == nullptr && h->one_pass != 2 && A->nnz >= kSampleMinNnz &&
+                         (h->one_pass == 0 || esc_mode == 0);
+    if (sampled) {
+        EscLimits el{};
+        for (int b = 0; b < kEscBins; b++) el.limit[b] = fil[b].limit;
+        const int32_t samples = std::min<int32_t>(m, kEscSamples);
+        cudaStream_t side = h->side[0];
+        ProductArgs ps = {};
+        ps.a_rpt = A->rpt;
+        ps.a_col = A->col;
+        ps.b_rpt = B->rpt;
+        ps.b_col = B->col;
+        ps.status = s.status;
+        if (cudaError_t e = cudaMemsetAsync(s.sample, 0, sizeof(EscSample), stream);
+            e != cudaSuccess)
+            return bail(cuda_fail(e, "reset the compression sample"));
+        if (cudaError_t e = cudaEventRecord(h->ev_fork, stream); e != cudaSuccess)
+            return bail(cuda_fail(e, "fork the sample stream"));
+        if (cudaError_t e = cudaStreamWaitEvent(side, h->ev_fork, 0); e != cudaSuccess)
+            return bail(cuda_fail(e, "fork the sample stream"));
+        B200_STEP(timed(h, "esc_sample", 0, -1, samples, side, [&](cudaStream_t ss) {
+            return launch_esc_sample(ps, m, samples, el, s.sample, ss);
+        }));
+        B200_STEP(timed(h, "esc_decide", 0, -1, 1, side, [&](cudaStream_t ss) {
+            return launch_esc_decide(s.sample, ladf, esc_mode, s.dladder, ss);
+        }));
+        if (cudaError_t e = cudaEventRecord(h->ev_sample, side); e != cudaSuccess)
+            return bail(cuda_fail(e, "join the sample stream"));
+    }
     B200_STEP(timed(h, "bin_offsets", 0, -1, m, stream, [&](cudaStream_t ss) {
         return launch_bin_offsets(s.hist1, nctas, nullptr, s.plan1, lad1, ss);
     }));
@@ -572,39 +612,26 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         // hashing (same limits, so the binning does not depend on it)
         BinLauncher one_fil[16];
         for (int b = 0; b < nfil && b < 16; b++) one_fil[b] = fil[b];
-        const bool esc_ok = narrow && h->esc != 2;
-        const bool esc_sampled = esc_ok && h->esc == 0;  // by the sample, if it ran
-        const Ladder ladf = make_ladder(fil, nfil, h->min_num_bin);
-        const bool sampled = (h->one_pass == 0 || esc_sampled) && A->nnz >= kSampleMinNnz;
-        if (sampled) {
-            // the compression sample reads A and B only: it runs on a side
-            // stream beside the fill binning and joins before the host sync
-            EscLimits el{};
-            for (int b = 0; b < kEscBins; b++) el.limit[b] = fil[b].limit;
-            const int32_t samples = std::min<int32_t>(m, kEscSamples);
-            cudaStream_t side = h->side[0];
-            B200_ONE_CUDA(cudaMemsetAsync(s.sample, 0, sizeof(EscSample), stream),
-                          "reset the compression sample");
-            B200_ONE_CUDA(cudaEventRecord(h->ev_fork, stream), "fork the sample stream");
-            B200_ONE_CUDA(cudaStreamWaitEvent(side, h->ev_fork, 0), "fork the sample stream");
-            B200_ONE(timed(h, "esc_sample", 2, -1, samples, side, [&](cudaStream_t ss) {
-                return launch_esc_sample(pa, m, samples, el, s.sample, ss);
-            }));
-            B200_ONE_CUDA(cudaEventRecord(h->ev_sample, side), "join the sample stream");
-        }
-        B200_ONE(timed(h, "nip_fill_hist", 2, -1, m, stream, [&](cudaStream_t ss) {
-            return launch_nnz_hist(off, m, s.hist2, s.cta_sum, s.plan2, ladf, ss);
-        }));
-        B200_ONE(timed(h, "nip_fill_offsets", 2, -1, m, stream, [&](cudaStream_t ss) {
-            return launch_bin_offsets(s.hist2, nctas, s.cta_sum, s.plan2, ladf, ss);
-        }));
-        B200_ONE(timed(h, "nip_fill_scatter", 2, -1, m, stream, [&](cudaStream_t ss) {
-            return launch_bin_scatter(off, m, s.hist2, s.cta_sum, s.bins2, s.plan2, ladf, true,
-                                      ss);
-        }));
-        mark(2);
+        const bool esc_ok = esc_mode != 2;
+        const bool esc_sampled = esc_mode == 0;  // by the sample, if it ran
+        // the fill binning's limits: decided on the device from the sample,
+        // or here when the sample did not run
+        Ladder ladh = ladf;
+        if (esc_mode == 1) ladh.limit[kEscBins - 1] = kEscSplit;
+        const Ladder* dlad = sampled ? s.dladder : nullptr;
         if (sampled)
             B200_ONE_CUDA(cudaStreamWaitEvent(stream, h->ev_sample, 0), "join the sample stream");
+        B200_ONE(timed(h, "nip_fill_hist", 2, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_nnz_hist(off, m, s.hist2, s.cta_sum, s.plan2, ladh, ss, dlad);
+        }));
+        B200_ONE(timed(h, "nip_fill_offsets", 2, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_bin_offsets(s.hist2, nctas, s.cta_sum, s.plan2, ladh, ss);
+        }));
+        B200_ONE(timed(h, "nip_fill_scatter", 2, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_bin_scatter(off, m, s.hist2, s.cta_sum, s.bins2, s.plan2, ladh, true,
+                                      ss, dlad);
+        }));
+        mark(2);
         B200_ONE(sync_mirror(h, stream, s.plan2, s, sampled));
         mark(3);
         B200_ONE(status_to_error(h->mirror->status));
@@ -634,11 +661,16 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         if (esc_ok) {
             const BinLauncher* esc = nullptr;
             const int nesc = sizeof(V) == 8 ? s2n_esc_ladder_f64(&esc) : s2n_esc_ladder_f32(&esc);
+            // the largest team bin and the 256-thread bin follow the device's
+            // decision (which also moved the split of their limits)
+            const bool split = esc_mode == 1 || (sampled && es.split != 0);
             for (int b = 0; b < kEscLadderBins && b < nesc && b < nfil; b++) {
-                const int sb = b < kEscBins ? b : kEscBins - 1;  // the CTA bin: the last team bin's sample
-                const bool use = !esc_sampled || (sampled && es.nnz[sb] > 0 &&
-                                                  static_cast<double>(es.nip[sb]) <=
-                                                      kEscMaxRatio[sb] * static_cast<double>(es.nnz[sb]));
+                const bool use =
+                    b >= kEscBins - 1
+                        ? split
+                        : (!esc_sampled || (sampled && es.nnz[b] > 0 &&
+                                            static_cast<double>(es.nip[b]) <=
+                                                kEscMaxRatio[b] * static_cast<double>(es.nnz[b])));
                 if (use) {
                     one_fil[b] = esc[b];
                     h->info.esc_mask |= 1 << b;
@@ -710,6 +742,12 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         }
 #undef B200_ONE_CUDA
 #undef B200_ONE
+    }
+    if (sampled && h->info.one_pass == 0) {
+        // two passes: the sample's work is not needed, but it still reads A
+        // and B; the final synchronisation must cover it
+        if (cudaError_t e = cudaStreamWaitEvent(stream, h->ev_sample, 0); e != cudaSuccess)
+            return bail(cuda_fail(e, "join the sample stream"));
     }
 
     // ---- sym1: exact nnz per row --------------------------------------------
