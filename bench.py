@@ -161,16 +161,57 @@ def replica_gflops(nip: int, steps: int, world: int, max_ms: float) -> float:
 # ---- clocks -----------------------------------------------------------------
 
 class ClockSampler:
+    """SM clock and clock-event reasons sampled DURING a timed region: NVML
+    polled every 5 ms from a thread (a timed region of a few steps lasts only
+    milliseconds); nvidia-smi at its 200 ms minimum if NVML is unavailable.
+    Reads only -- no setting of the GPU is touched."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+               "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+               "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+               "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.samples = []  # (sm MHz, max MHz, reason bits) from NVML
+        self.stop = threading.Event()
+        self.nvml = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
+        ident = vis[self.gpu].strip() if self.gpu < len(vis) and vis[self.gpu].strip() else None
+        if ident is None:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+        if ident.isdigit():
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(int(ident))
+        return pynvml, pynvml.nvmlDeviceGetHandleByUUID(ident)
+
+    def _poll(self, nv, hd):
+        mx = nv.nvmlDeviceGetMaxClockInfo(hd, nv.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(hd, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(hd)
+                self.samples.append((float(sm), float(mx), int(rs)))
+            except Exception:
+                pass
+            self.stop.wait(0.005)
 
     def __enter__(self):
+        try:
+            nv, hd = self._nvml_handle()
+            self.nvml = nv
+            self.t = threading.Thread(target=self._poll, args=(nv, hd), daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
@@ -187,6 +228,10 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        if self.nvml is not None:
+            self.stop.set()
+            self.t.join(timeout=2)
+            return
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -196,23 +241,34 @@ class ClockSampler:
 
     def summary(self):
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
+        if self.nvml is not None:
+            for s_mhz, m_mhz, bits in self.samples:
+                sm.append(s_mhz)
+                mx = m_mhz
+                for nm, const in self.REASONS.items():
+                    if bits & int(getattr(self.nvml, const, 0)):
+                        reasons.add(nm)
+            source = "nvml, 5 ms"
+        else:
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for ln in self.lines:
+                parts = [p.strip() for p in ln.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+            source = "nvidia-smi, 200 ms"
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "source": source}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": source}
 
 
 # ---- the reference arm: CPU restatement on the host cores -------------------
