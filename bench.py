@@ -62,7 +62,10 @@ TRAFFIC_PER_ALG_BYTE = {
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 50 for the plain product, whose step "
+                         "takes ~1.4 ms, so that clocks are sampled inside the region; "
+                         "10 for the other modes)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--dtype", choices=["f64", "f32"], default="f64")
@@ -209,6 +212,10 @@ class ClockSampler:
             self.nvml = nv
             self.t = threading.Thread(target=self._poll, args=(nv, hd), daemon=True)
             self.t.start()
+            t0 = time.perf_counter()  # polling before the region starts
+            while not self.samples and time.perf_counter() - t0 < 1.0:
+                time.sleep(0.001)
+            self.samples.clear()
             return self
         except Exception:
             self.nvml = None
@@ -841,6 +848,8 @@ def run_served(args, local_rank):
 
 def main():
     args = parse()
+    if args.steps is None:
+        args.steps = 50 if args.mode == "plain" and args.impl == "ours" else 10
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
