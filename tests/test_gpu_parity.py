@@ -260,8 +260,16 @@ def test_esc_chosen_by_sampled_compression(handle, oracle_mod):
     try:
         P = G.power_law(30000, 2.0, 3000, seed=21)
         C = gpu_product(P, P, handle, np.float64)
-        assert handle.info()["esc_mask"] == 0b11111
+        info = handle.info()
+        assert info["esc_mask"] == 0b11111
         check(oracle_mod, P, P, C, np.float64, "esc_auto_power_law", positive=True)
+        # with both expanding, the 32-lane / 256-thread split moved to 512
+        # products (decided on the device): bin 3 holds rows of 193-512
+        # products, bin 4 rows of 513-3,072
+        nip = oracle_mod.nip(P, P, per_row=True)[1]
+        assert info["num_bin_rows"][3] == int(((nip > 192) & (nip <= 512)).sum())
+        assert info["num_bin_rows"][4] == int(((nip > 512) & (nip <= 3072)).sum())
+        assert int(((nip > 512) & (nip <= 768)).sum()) > 0
         S = G.stencil27(12)
         C = gpu_product(S, S, handle, np.float64)
         assert handle.info()["esc_mask"] == 0
