@@ -114,6 +114,10 @@ constexpr double kEscMaxRatio[kEscBins] = {8.0, 8.0, 1.4, 1.1};
 constexpr int kEscLadderBins = kEscBins + 1;
 // The sample runs for products with at least this many entries in A.
 constexpr int64_t kSampleMinNnz = int64_t(1) << 16;
+// Products with at least this many entries in A are expected to run one pass:
+// they are binned for the fill right after the NIP pass, before the first
+// synchronisation (the count binning follows only if they run two).
+constexpr int64_t kEarlyOnePassNnz = int64_t(1) << 18;
 // Auto mode keeps two passes when at least this share of the sampled NIP
 // lies in rows above the team bins (one pass bins them by NIP into the CTA
 // bins, two passes by nnz into small team tables) and the team bins' sampled

@@ -78,6 +78,7 @@ struct ProfRec {
 // Pinned host mirror of the device-side plan words, copied in one transfer.
 struct HostMirror {
     Plan plan;
+    Plan plan_b;  // a second plan, when one synchronisation reads two
     DevStatus status;
     int32_t fail_count;
     int32_t pad[3];
@@ -106,6 +107,8 @@ struct spgemm_handle_s {
     // (products of different shapes in turn, as in R * (A * P)).
     void* onepass = nullptr;
     size_t onepass_bytes = 0;
+    void* slots = nullptr;  // one-pass NIP slot starts (m + 1), grown like the rest
+    size_t slots_bytes = 0;
     b200::HostMirror* mirror = nullptr;  // pinned
     // host-operand staging on the device
     void* in_buf = nullptr;
@@ -271,7 +274,11 @@ spgemm_status status_to_error(const DevStatus& st) {
 }
 
 spgemm_status sync_mirror(spgemm_handle_s* h, cudaStream_t stream, const Plan* plan,
-                          const Scratch& s, bool with_sample = false) {
+                          const Scratch& s, bool with_sample = false,
+                          const Plan* plan_b = nullptr) {
+    if (plan_b != nullptr)
+        B200_TRY(cudaMemcpyAsync(&h->mirror->plan_b, plan_b, sizeof(Plan), cudaMemcpyDeviceToHost,
+                                 stream));
     if (with_sample)
         B200_TRY(cudaMemcpyAsync(&h->mirror->sample, s.sample, sizeof(EscSample),
                                  cudaMemcpyDeviceToHost, stream));
@@ -447,6 +454,11 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         spgemm_status st_ = (expr);                                      \
         if (st_ != SPGEMM_OK) return bail(st_);                          \
     } while (0)
+#define B200_STEP_R(expr)                                                \
+    do {                                                                 \
+        spgemm_status st_ = (expr);                                      \
+        if (st_ != SPGEMM_OK) return st_;                                \
+    } while (0)
 
     Scratch s;
     B200_STEP(ensure_scratch(h, m, &s, stream));
@@ -521,20 +533,62 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         if (cudaError_t e = cudaEventRecord(h->ev_sample, side); e != cudaSuccess)
             return bail(cuda_fail(e, "join the sample stream"));
     }
-    B200_STEP(timed(h, "bin_offsets", 0, -1, m, stream, [&](cudaStream_t ss) {
-        return launch_bin_offsets(s.hist1, nctas, nullptr, s.plan1, lad1, ss);
-    }));
-    B200_STEP(timed(h, "bin_scatter", 0, -1, m, stream, [&](cudaStream_t ss) {
-        return launch_bin_scatter(c_rpt, m, s.hist1, nullptr, s.bins1, s.plan1, lad1, false, ss);
-    }));
+    // The fill binning by NIP (the one-pass path's), with limits decided on
+    // the device when the sample ran: off = the scan of the NIP per row.
+    int32_t* off = nullptr;
+    Ladder ladh = ladf;
+    if (esc_mode == 1) ladh.limit[kEscBins - 1] = kEscSplit;
+    const Ladder* dlad = sampled ? s.dladder : nullptr;
+    auto fill_binning = [&]() -> spgemm_status {
+        B200_STEP_R(regrow(h, &h->slots, &h->slots_bytes, sizeof(int32_t) * (size_t(m) + 1),
+                           stream));
+        off = static_cast<int32_t*>(h->slots);
+        B200_TRY(cudaMemcpyAsync(off, c_rpt, sizeof(int32_t) * size_t(m), cudaMemcpyDeviceToDevice,
+                                 stream));
+        if (sampled) B200_TRY(cudaStreamWaitEvent(stream, h->ev_sample, 0));
+        B200_STEP_R(timed(h, "nip_fill_hist", 2, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_nnz_hist(off, m, s.hist2, s.cta_sum, s.plan2, ladh, ss, dlad);
+        }));
+        B200_STEP_R(timed(h, "nip_fill_offsets", 2, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_bin_offsets(s.hist2, nctas, s.cta_sum, s.plan2, ladh, ss);
+        }));
+        B200_STEP_R(timed(h, "nip_fill_scatter", 2, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_bin_scatter(off, m, s.hist2, s.cta_sum, s.bins2, s.plan2, ladh, true, ss,
+                                      dlad);
+        }));
+        return SPGEMM_OK;
+    };
+    // The count binning by NIP (the two-pass path's).
+    auto count_binning = [&]() -> spgemm_status {
+        B200_STEP_R(timed(h, "bin_offsets", 0, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_bin_offsets(s.hist1, nctas, nullptr, s.plan1, lad1, ss);
+        }));
+        B200_STEP_R(timed(h, "bin_scatter", 0, -1, m, stream, [&](cudaStream_t ss) {
+            return launch_bin_scatter(c_rpt, m, s.hist1, nullptr, s.bins1, s.plan1, lad1, false,
+                                      ss);
+        }));
+        return SPGEMM_OK;
+    };
+    // A product likely to run one pass is binned for the fill right away and
+    // decided at the one synchronisation that follows; the count binning then
+    // runs only if it turns out two-pass.
+    const bool early = cr == nullptr && h->one_pass != 2 &&
+                       (h->one_pass == 1 || A->nnz >= kEarlyOnePassNnz);
+    if (early) {
+        B200_STEP(fill_binning());
+    } else {
+        B200_STEP(count_binning());
+    }
     mark(0);
-    B200_STEP(sync_mirror(h, stream, s.plan1, s));
+    B200_STEP(sync_mirror(h, stream, s.plan1, s, early && sampled, early ? s.plan2 : nullptr));
     mark(1);
     B200_STEP(status_to_error(h->mirror->status));
-    const Plan p1 = h->mirror->plan;
+    Plan p1 = h->mirror->plan;  // bin sizes valid once the count binning ran
     h->info.nip = p1.total_key;
     h->info.max_row_nip = p1.max_key;
-    for (int b = 0; b < nsym && b < 16; b++) h->info.sym_bin_rows[b] = p1.bin_size[b];
+    bool counted = !early;
+    if (counted)
+        for (int b = 0; b < nsym && b < 16; b++) h->info.sym_bin_rows[b] = p1.bin_size[b];
 
     ProductArgs pa = {};
     pa.a_rpt = A->rpt;
@@ -572,7 +626,6 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
           static_cast<uint64_t>(nip_total) * (4 + sizeof(V)) <= kOnePassMaxBytes));
     h->info.one_pass = one_pass ? 1 : 0;
     if (one_pass) {
-        int32_t* off = nullptr;
         int32_t* tmp_col = nullptr;
         void* tmp_val = nullptr;
         auto release = [&]() {};
@@ -592,50 +645,20 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
             return bail(cuda_fail(e_, what));                            \
         }                                                                \
     } while (0)
-        // NIP slots: the scan of the NIP per row (c_rpt holds it) into off
-        {
-            // off (m + 1 slot starts), tmp_col (NIP + 4 columns: a row's tail
-            // never leaves the buffer), tmp_val (NIP values), 256-byte aligned
-            const size_t o_col = align_up(sizeof(int32_t) * (size_t(m) + 1), 256);
-            const size_t o_val = align_up(o_col + sizeof(int32_t) * size_t(nip_total) + 16, 256);
-            const size_t need = o_val + sizeof(V) * size_t(nip_total);
-            B200_ONE(regrow(h, &h->onepass, &h->onepass_bytes, need, stream));
-            char* base = static_cast<char*>(h->onepass);
-            off = reinterpret_cast<int32_t*>(base);
-            tmp_col = reinterpret_cast<int32_t*>(base + o_col);
-            tmp_val = base + o_val;
-        }
-        B200_ONE_CUDA(cudaMemcpyAsync(off, c_rpt, sizeof(int32_t) * size_t(m),
-                                      cudaMemcpyDeviceToDevice, stream),
-                      "copy NIP per row");
-        // B.n <= 2^20: team bins may expand, sort and compress instead of
+        // B.n <= 2^20: fill bins may expand, sort and compress instead of
         // hashing (same limits, so the binning does not depend on it)
         BinLauncher one_fil[16];
         for (int b = 0; b < nfil && b < 16; b++) one_fil[b] = fil[b];
         const bool esc_ok = esc_mode != 2;
         const bool esc_sampled = esc_mode == 0;  // by the sample, if it ran
-        // the fill binning's limits: decided on the device from the sample,
-        // or here when the sample did not run
-        Ladder ladh = ladf;
-        if (esc_mode == 1) ladh.limit[kEscBins - 1] = kEscSplit;
-        const Ladder* dlad = sampled ? s.dladder : nullptr;
-        if (sampled)
-            B200_ONE_CUDA(cudaStreamWaitEvent(stream, h->ev_sample, 0), "join the sample stream");
-        B200_ONE(timed(h, "nip_fill_hist", 2, -1, m, stream, [&](cudaStream_t ss) {
-            return launch_nnz_hist(off, m, s.hist2, s.cta_sum, s.plan2, ladh, ss, dlad);
-        }));
-        B200_ONE(timed(h, "nip_fill_offsets", 2, -1, m, stream, [&](cudaStream_t ss) {
-            return launch_bin_offsets(s.hist2, nctas, s.cta_sum, s.plan2, ladh, ss);
-        }));
-        B200_ONE(timed(h, "nip_fill_scatter", 2, -1, m, stream, [&](cudaStream_t ss) {
-            return launch_bin_scatter(off, m, s.hist2, s.cta_sum, s.bins2, s.plan2, ladh, true,
-                                      ss, dlad);
-        }));
-        mark(2);
-        B200_ONE(sync_mirror(h, stream, s.plan2, s, sampled));
+        if (!early) {
+            B200_ONE(fill_binning());
+            mark(2);
+            B200_ONE(sync_mirror(h, stream, s.plan2, s, sampled, s.plan2));
+        }
         mark(3);
         B200_ONE(status_to_error(h->mirror->status));
-        const Plan pf = h->mirror->plan;
+        const Plan pf = h->mirror->plan_b;
         const EscSample es = h->mirror->sample;
         // sampled: the NIP of rows above the team bins, the team bins' NIP/nnz
         int64_t team_nip = 0;
@@ -650,11 +673,19 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
                 kTwoPassMinShare * static_cast<double>(es.nip_seen) &&
             static_cast<double>(team_nip) >= kTwoPassMinRatio * static_cast<double>(team_nnz);
         if (h->one_pass == 0 && wide_rows_compress) {
-            // two passes after all: C.rpt still holds the NIP per row; the
-            // fill binning's plan is reused by the scan pass
+            // two passes after all: C.rpt still holds the NIP per row
             h->info.one_pass = 0;
-            B200_ONE_CUDA(cudaMemsetAsync(s.plan2, 0, sizeof(Plan), stream), "reset a plan");
         } else {
+        // NIP-sized temporaries: tmp_col (NIP + 4 columns: a row's tail never
+        // leaves the buffer) and tmp_val (NIP values), 256-byte aligned
+        {
+            const size_t o_val = align_up(sizeof(int32_t) * size_t(nip_total) + 16, 256);
+            const size_t need = o_val + sizeof(V) * size_t(nip_total);
+            B200_ONE(regrow(h, &h->onepass, &h->onepass_bytes, need, stream));
+            char* base = static_cast<char*>(h->onepass);
+            tmp_col = reinterpret_cast<int32_t*>(base);
+            tmp_val = base + o_val;
+        }
         // C.rpt receives each row's exact nnz (rows without products stay 0)
         B200_ONE_CUDA(cudaMemsetAsync(c_rpt, 0, sizeof(int32_t) * (size_t(m) + 1), stream),
                       "memset row counts");
@@ -730,9 +761,6 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
             }));
         }
         release();
-        off = nullptr;
-        tmp_col = nullptr;
-        tmp_val = nullptr;
         if (cudaError_t e = cudaStreamSynchronize(stream); e != cudaSuccess)
             return bail(cuda_fail(e, "final synchronize"));
         mark(6);
@@ -748,6 +776,19 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         // and B; the final synchronisation must cover it
         if (cudaError_t e = cudaStreamWaitEvent(stream, h->ev_sample, 0); e != cudaSuccess)
             return bail(cuda_fail(e, "join the sample stream"));
+    }
+    if (early || one_pass) {
+        // the fill binning by NIP ran: its plan is reused by the scan pass
+        if (cudaError_t e = cudaMemsetAsync(s.plan2, 0, sizeof(Plan), stream); e != cudaSuccess)
+            return bail(cuda_fail(e, "reset a plan"));
+    }
+    if (!counted) {
+        // a product binned early for one pass runs two: its count binning now
+        B200_STEP(count_binning());
+        B200_STEP(sync_mirror(h, stream, s.plan1, s));
+        B200_STEP(status_to_error(h->mirror->status));
+        p1 = h->mirror->plan;
+        for (int b = 0; b < nsym && b < 16; b++) h->info.sym_bin_rows[b] = p1.bin_size[b];
     }
 
     // ---- sym1: exact nnz per row --------------------------------------------
@@ -1764,6 +1805,7 @@ spgemm_status spgemm_destroy(spgemm_handle_t h) {
     if (h->scratch) cudaFree(h->scratch);
     if (h->bitmaps) cudaFree(h->bitmaps);
     if (h->onepass) cudaFree(h->onepass);
+    if (h->slots) cudaFree(h->slots);
     if (h->in_buf) cudaFree(h->in_buf);
     if (h->mirror) cudaFreeHost(h->mirror);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);

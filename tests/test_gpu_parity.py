@@ -365,7 +365,9 @@ def test_one_pass_chosen_and_equal_to_two_pass(handle, oracle_mod):
         info2 = handle.info()
     finally:
         handle.set_option(N.OPT_ONE_PASS, 0)
-    assert info2["one_pass"] == 0 and info2["host_syncs"] == 3 and info1["host_syncs"] == 4
+    # one pass, binned for the fill before the first synchronisation: NIP +
+    # fill binning, row counts, final; two passes: NIP binning, scan, final
+    assert info2["one_pass"] == 0 and info2["host_syncs"] == 3 and info1["host_syncs"] == 3
     assert np.array_equal(C1.rpt, C2.rpt) and np.array_equal(C1.col, C2.col)
     assert info1["nnz"] == info2["nnz"] and info1["max_row_nnz"] == info2["max_row_nnz"]
     check(oracle_mod, A, A, C1, np.float64, "one_pass_default", positive=True)
