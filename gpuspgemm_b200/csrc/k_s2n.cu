@@ -261,10 +261,11 @@ __global__ __launch_bounds__(THREADS) void k_esc_cta(ProductArgs p) {
 }
 
 // Compression of the team bins, sampled: `samples` rows spread evenly over
-// A are counted exactly (one warp per row, a 1024-slot shared hash set) when
-// their NIP is at most the last team bin's limit, and their NIP and nnz are
-// summed per team bin (binned by NIP with the ladder's limits); the NIP of
-// the longer sampled rows is summed apart.  It needs A and B only, so it runs
+// A are counted exactly over their first kSampleProducts products (one warp
+// per row, a 1024-slot shared hash set) when their NIP is at most the last
+// team bin's limit, and those products and their distinct columns are summed
+// per team bin (binned by NIP with the ladder's limits); the NIP of every
+// sampled row, and of the longer ones apart, is summed too.  It needs A and B only, so it runs
 // on a side stream beside the NIP pass; the host reads the sums with the NIP
 // plan.  They choose one pass or two (rows above the team bins that repeat
 // many columns fill small nnz-sized tables only in two passes) and let a
@@ -272,6 +273,7 @@ __global__ __launch_bounds__(THREADS) void k_esc_cta(ProductArgs p) {
 // sorts every product, the hash bins only the distinct columns.
 constexpr int kSampleWarps = 8;
 constexpr int kSampleSlots = 1024;
+constexpr int kSampleProducts = 256;  // products counted per sampled row
 
 __global__ __launch_bounds__(kSampleWarps * kWarp) void k_esc_sample(ProductArgs p, int32_t m,
                                                                       int32_t samples,
@@ -311,11 +313,33 @@ __global__ __launch_bounds__(kSampleWarps * kWarp) void k_esc_sample(ProductArgs
     if (nip > cap || nip > 3 * kSampleSlots / 4) return;
     int b = 0;
     while (nip > lim.limit[b]) b++;
+    // count the row's first kSampleProducts products only (the walk's latency
+    // is the sample's cost): the A entries up to the one that reaches them
+    int a_cut = a1;
+    if (nip > kSampleProducts) {
+        int run = 0;
+        for (int base = a0; base < a1; base += kWarp) {
+            const int e = base + lane;
+            int len = 0;
+            if (e < a1) {
+                const int c = __ldg(p.a_col + e);
+                len = __ldg(p.b_rpt + c + 1) - __ldg(p.b_rpt + c);
+            }
+            const int inc = team_inclusive_scan<kWarp>(0xffffffffu, len, lane);
+            const unsigned hit = __ballot_sync(0xffffffffu, run + inc >= kSampleProducts);
+            if (hit != 0u) {
+                a_cut = base + __ffs(hit);
+                break;
+            }
+            run += __shfl_sync(0xffffffffu, inc, kWarp - 1);
+        }
+    }
     int32_t* tab = s_tab[wid];
     for (int i = lane; i < kSampleSlots; i += kWarp) tab[i] = kEmpty;
     __syncwarp();
-    team_for_products<kWarp>(p.a_col, p.b_rpt, a0, a1, [&](int qb, int) {
-        table_insert(tab, kSampleSlots, __ldg(p.b_col + qb), p.status, row);
+    team_for_products_at<kWarp>(p.a_col, p.b_rpt, a0, a_cut, [&](int qb, int, int q) {
+        if (q < kSampleProducts)
+            table_insert(tab, kSampleSlots, __ldg(p.b_col + qb), p.status, row);
     });
     __syncwarp();
     int cnt = 0;
@@ -324,7 +348,7 @@ __global__ __launch_bounds__(kSampleWarps * kWarp) void k_esc_sample(ProductArgs
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if (lane == 0) {
         atomicAdd(reinterpret_cast<unsigned long long*>(&out->nip[b]),
-                  static_cast<unsigned long long>(nip));
+                  static_cast<unsigned long long>(min(nip, kSampleProducts)));
         atomicAdd(reinterpret_cast<unsigned long long*>(&out->nnz[b]),
                   static_cast<unsigned long long>(cnt));
     }
