@@ -428,6 +428,18 @@ def test_dimension_mismatch_raises(handle):
         gpu_product(A, B, handle, np.float64)
 
 
+def test_mode_options_validated(handle):
+    """The pass and expand-sort-compress modes take 0, 1 or 2 only; a bad
+    value is rejected and the option keeps its value."""
+    from gpuspgemm_b200 import SpgemmError
+    from gpuspgemm_b200 import _native as N
+    for opt in (N.OPT_ONE_PASS, N.OPT_ESC):
+        for bad in (-1, 3):
+            with pytest.raises(SpgemmError, match="INVALID_ARG"):
+                handle.set_option(opt, bad)
+        assert handle.get_option(opt) == 0
+
+
 def test_checked_mode_rejects_unsorted(handle):
     from gpuspgemm_b200 import SpgemmError
     from gpuspgemm_b200 import _native as N
