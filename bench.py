@@ -34,29 +34,18 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "C=A*A GFLOPS (2*NIP/s), power-law n=1e6 FP64"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic
-# byte of the fill kernels, from one ncu capture of the power-law n = 200,000
-# case (profiles/s2n_fused_powerlaw200k_f64.md; ncu runs each launch from cold
-# caches): the kernel's DRAM bytes over the algorithmic bytes of the same
-# launch, as this bench computes them for that case.  The bench scales the
-# ratio to the launch it reports by that launch's algorithmic bytes: at both
-# sizes A and B fit in L2, so DRAM reads are the first touch of the A and B
-# rows a bin reads, and C's writes drain from L2 after the kernel.
-TRAFFIC_PER_ALG_BYTE = {
-    "s2n_team4_t16": 11508224 / 14947704,
-    "s2n_team8_t64": 10017792 / 11855028,
-    "s2n_team16_t256": 10184960 / 16517676,
-    "s2n_team32_t1024": 10851840 / 20804236,
-    "s2n_cta256_t4096": 11505152 / 24898604,
-    # one-pass expand-sort-compress bins (rows keyed by NIP), same n = 200k case
-    "esc_team4_n12": 9732864 / 14947704,
-    "esc_team8_n48": 8819456 / 11855028,
-    "esc_team16_n192": 9604608 / 16511032,
-    "esc_team32_n768": 10614272 / 20784028,
-}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of a
+# fill kernel on the default workload (the power-law n = 1e6 product, seed
+# 20261203), from an ncu capture of that kernel alone on that product
+# (`-k <kernel> -c 1`, cold caches): key (kernel, value dtype).  Other
+# workloads report traffic null.
+MEASURED_TRAFFIC = {}
+
+
+def metric_name(dtype: str) -> str:
+    return f"C=A*A GFLOPS (2*NIP/s), power-law n=1e6 {dtype.upper()}"
 
 
 def parse():
@@ -73,7 +62,8 @@ def parse():
     ap.add_argument("--exponent", type=float, default=2.0)
     ap.add_argument("--cap", type=int, default=4700)
     ap.add_argument("--seed", type=int, default=20261203)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=None,
+                    help="end-to-end steps (default: as many as --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--out", type=str, default="")
     ap.add_argument("--mode", choices=["plain", "batch", "served", "galerkin"], default="plain",
@@ -300,7 +290,7 @@ def run_reference(args, rank):
     total = sum(times)
     gflops = 2.0 * nip * args.steps / total / 1e9
     line = {
-        "metric": METRIC, "value": gflops, "unit": "GFLOPS", "n_gpus": args.gpus,
+        "metric": metric_name(args.dtype), "value": gflops, "unit": "GFLOPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": args.dtype, "data": "synthetic (seeded generator)",
@@ -342,11 +332,10 @@ def run_ours(args, rank, world, local_rank):
     nip = info["nip"]
     nnz_c = info["nnz"]
 
-    h.set_option(N.OPT_PROFILE, 1)
+    # the timed region: plain products, no per-launch events (the library's
+    # default side streams; L2 flushed before every step, outside its events)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    kernel_ms = {}
-    launches = 0
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -357,16 +346,34 @@ def run_ours(args, rank, world, local_rank):
             C = proposal(dA, dA, h)
             ends[i].record(stream)
             del C
-            for k in h.profile():
-                key = (k["phase"], k["bin"], k["name"])
-                kernel_ms.setdefault(key, []).append(k["ms"])
-                launches += 1
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = max_over_ranks(float(sum(step_ms)), world, dev)
+
+    # per-kernel times for the roofline, in a pass of its own: one side
+    # stream, so every launch runs alone and its event pair times it alone
+    # (the timed region runs the fill bins side by side on several streams,
+    # where an event pair also spans other bins' work)
+    nside = h.get_option(N.OPT_STREAMS)
+    h.set_option(N.OPT_STREAMS, 1)
+    h.set_option(N.OPT_PROFILE, 1)
+    kernel_ms = {}
+    launches_per_step = 0
+    serial_steps = 5
+    for i in range(serial_steps):
+        flush.fill_(float(i))
+        C = proposal(dA, dA, h)
+        del C
+        recs = h.profile()
+        launches_per_step = len(recs)
+        for k in recs:
+            kernel_ms.setdefault((k["phase"], k["bin"], k["name"]), []).append(k["ms"])
+    torch.cuda.synchronize()
     h.set_option(N.OPT_PROFILE, 0)
+    h.set_option(N.OPT_STREAMS, nside)
+    launches = launches_per_step * args.steps
 
     value = replica_gflops(nip, args.steps, world, total_ms)
     phase_us = h.info()["phase_us"]
@@ -396,14 +403,15 @@ def run_ours(args, rank, world, local_rank):
     from gpuspgemm_b200.csr import HostCSR
     Ap = HostCSR(A.m, A.n, pin["rpt"].numpy(), pin["col"].numpy(), pin["val"].numpy())
     s_bytes = 8 if args.dtype == "f64" else 4
-    h2d = 2 * (4 * (A.m + 1) + (4 + s_bytes) * A.nnz)
+    h2d = 4 * (A.m + 1) + (4 + s_bytes) * A.nnz  # A once: C = A*A passes one host matrix
     d2h = 4 * (A.m + 1) + (4 + s_bytes) * nnz_c
     Ch = proposal_host(Ap, Ap, h)  # warm (grows the input staging)
     del Ch
     e2e_ms = []
     if world > 1:
         dist.barrier()
-    for _ in range(args.e2e_steps):
+    e2e_steps = args.steps if args.e2e_steps is None else args.e2e_steps
+    for _ in range(e2e_steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         Ch = proposal_host(Ap, Ap, h)
@@ -411,16 +419,19 @@ def run_ours(args, rank, world, local_rank):
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
         del Ch
     e2e_total = max_over_ranks(float(sum(e2e_ms)) if e2e_ms else float("nan"), world, dev)
-    e2e_value = replica_gflops(nip, args.e2e_steps, world, e2e_total) if e2e_ms else None
+    e2e_value = replica_gflops(nip, e2e_steps, world, e2e_total) if e2e_ms else None
 
     if rank != 0:
         h.close()
         return None
 
-    # roofline of the dominant kernel
+    # roofline of the dominant kernel: the longest launch of the serialised pass
     avg = {k: float(np.mean(v)) for k, v in kernel_ms.items()}
     dom = max(avg, key=avg.get)
     phase, b, name = dom
+    default_workload = (args.n, args.exponent, args.cap, args.seed) == (1_000_000, 2.0, 4700,
+                                                                       20261203)
+    traffic = MEASURED_TRAFFIC.get((name, args.dtype)) if default_workload else None
     # per-row NIP (numpy) and nnz (the library's own C.rpt) for the byte model
     deg = np.diff(A.rpt).astype(np.int64)
     contrib = deg[A.col]
@@ -459,16 +470,18 @@ def run_ours(args, rank, world, local_rank):
         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
         "peak_source": "MEASURED_PEAKS.json" if PEAKS_FILE.exists() else "fallback",
         "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg[dom],
-        "traffic": (TRAFFIC_PER_ALG_BYTE[name] * alg_bytes if name in TRAFFIC_PER_ALG_BYTE
-                    else None),
-        "traffic_source": ("ncu dram bytes of the n=200k case, scaled by algorithmic bytes"
-                           if name in TRAFFIC_PER_ALG_BYTE else None),
+        "traffic": traffic,
+        "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel "
+                           "on this product (one launch, cold caches)" if traffic else None),
+        "timing": f"serialised pass: one side stream, {serial_steps} products, CUDA event "
+                  "pair around every launch; the timed steps run side streams concurrently",
         "whole_product": {"alg_bytes": whole_bytes,
                           "achieved_gbs": whole_bytes / (step_ms_avg / 1e3) / 1e9},
     }
-    kernels = sorted(({"kernel": k[2], "phase": k[0], "bin": k[1], "avg_ms": avg[k],
-                       "share": avg[k] / max(step_ms_avg, 1e-9)} for k in avg),
-                     key=lambda r: -r["avg_ms"])
+    serial_total = sum(avg.values())
+    kernels = sorted(({"kernel": k[2], "phase": k[0], "bin": k[1], "serial_ms": avg[k],
+                       "share_of_serial": avg[k] / max(serial_total, 1e-9)} for k in avg),
+                     key=lambda r: -r["serial_ms"])
 
     cpu = None
     if not args.no_cpu_baseline:
@@ -487,19 +500,21 @@ def run_ours(args, rank, world, local_rank):
                "sample": "the full workload, median of 3 (row-wise Gustavson, OpenMP)"}
 
     line = {
-        "metric": METRIC, "value": value, "unit": "GFLOPS", "n_gpus": world,
+        "metric": metric_name(args.dtype), "value": value, "unit": "GFLOPS", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": args.dtype, "data": "synthetic (seeded generator)",
         "config": config_of(args, A, nip, nnz_c),
         "e2e": {"value": e2e_value, "unit": "GFLOPS", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
-                "ms_per_step": e2e_total / args.e2e_steps if e2e_ms else None},
+                "ms_per_step": e2e_total / e2e_steps if e2e_ms else None,
+                "steps": e2e_steps},
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": launches,
         "kernels": kernels[:12],
+        "serial_kernel_ms_per_step": serial_total,
         "host_syncs_per_step": info["host_syncs"],
         "host_phase_us_last_step": phase_us,
         "plan_replay": {"ms": plan_replay_ms, "gflops": 2.0 * nip / (plan_replay_ms / 1e3) / 1e9,

@@ -133,7 +133,16 @@ __global__ __launch_bounds__(THREADS) void k_esc_team(ProductArgs p) {
     team_for_products_at<G>(p.a_col, p.b_rpt, p.a_rpt[row], p.a_rpt[row + 1],
                             [&](int qb, int ai, int q) {
                                 if (q < NMAX) {
-                                    keys[q] = (__ldg(p.b_col + qb) << SHIFT) | q;
+                                    int32_t col = __ldg(p.b_col + qb);
+                                    // a column outside [0, B.n) would corrupt
+                                    // the packed key: report it, keep the key
+                                    // in range
+                                    if (static_cast<uint32_t>(col) >=
+                                        static_cast<uint32_t>(p.n_cols)) {
+                                        report(p.status, kStBadInput, row, col);
+                                        col = 0;
+                                    }
+                                    keys[q] = (col << SHIFT) | q;
                                     vals[q] = ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb);
                                 }
                             });
@@ -599,10 +608,12 @@ __global__ __launch_bounds__(THREADS) void k_s2n_global(ProductArgs p) {
         V* out = static_cast<V*>(p.c_val) + c0;
         for (int i = threadIdx.x; i < nnz; i += THREADS) out[i] = V(0);
         __syncthreads();
+        if (nnz == 0) continue;  // only skipped (invalid) keys: nothing to add into
         cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int ai) {
             const int32_t key = __ldg(p.b_col + qb);
             const int pos = lower_bound_present(cols, nnz, key);
-            atomicAdd(out + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
+            // a key that was skipped above (outside [0, B.n)) is not in the row
+            if (cols[pos] == key) atomicAdd(out + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
         });
     }
 }

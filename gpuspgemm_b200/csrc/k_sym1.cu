@@ -13,6 +13,7 @@
 //   global bin  fail-list rows: a bitmap over B's columns in global memory
 #include <cooperative_groups.h>
 
+#include "cluster_insert.cuh"
 #include "cta.cuh"
 #include "kernels.hpp"
 
@@ -66,73 +67,86 @@ __global__ __launch_bounds__(THREADS) void k_sym1_cta(ProductArgs p) {
 // global table lives in CTA h / T of the cluster at local slot h % T, reached
 // through distributed shared memory (ld/st/atom.shared::cluster; no TMA).
 // The CTAs of the cluster share the row's products.  A row whose distinct
-// count passes 80 % of the cluster capacity stops and goes to the fail list
-// (the reference's k_sym1_smem_max does the same per CTA, sym1.cuh:171-245).
+// count passes 80 % of the cluster capacity, or one of whose keys probes
+// kClusterMaxProbes slots, stops and goes to the fail list (the reference's
+// k_sym1_smem_max spills per CTA on its per-insert load test,
+// sym1.cuh:171-245).  The insert and its bounds are cluster_insert.cuh's.
+struct ClusterTableOps {
+    cg::cluster_group cluster;
+    int32_t* table;      // this CTA's T slots (the same offset in every CTA)
+    int32_t* s_count;    // this CTA's new-key count
+    int32_t* s_spill;    // this CTA's copy of the row's spill flag
+    int32_t* s_total;    // the published total (read through CTA 0)
+    uint32_t T;
+    uint32_t nslots;
+    int32_t load_limit;
+    int32_t ncta;
+
+    __device__ uint32_t slots() const { return nslots; }
+    __device__ int32_t empty() const { return kEmpty; }
+    __device__ int32_t limit() const { return load_limit; }
+    __device__ int32_t csize() const { return ncta; }
+    __device__ int32_t cas(uint32_t h, int32_t key) {
+        int32_t* slot = cluster.map_shared_rank(table + (h % T), static_cast<int>(h / T));
+        return atomicCAS(slot, kEmpty, key);
+    }
+    __device__ bool spilled() { return *reinterpret_cast<volatile int32_t*>(s_spill) != 0; }
+    __device__ void spill() {
+        for (int r = 0; r < ncta; r++) atomicExch(cluster.map_shared_rank(s_spill, r), 1);
+    }
+    __device__ int32_t count_local() { return atomicAdd(s_count, 1); }
+    __device__ int32_t publish(int32_t add) {
+        return atomicAdd(cluster.map_shared_rank(s_total, 0), add) + add;
+    }
+};
+
 template<int THREADS, int T>
 __global__ __launch_bounds__(THREADS) void k_sym1_cluster(ProductArgs p) {
     extern __shared__ int32_t smem[];
     auto& sc = *reinterpret_cast<CtaScratch<THREADS>*>(smem + T);
     __shared__ int32_t s_count;   // distinct keys inserted by this CTA
-    __shared__ int32_t s_abort;   // cluster-wide abort flag (lives in CTA 0)
+    __shared__ int32_t s_spill;   // the row's spill flag (every CTA holds a copy)
+    __shared__ int32_t s_total;   // published count (used in CTA 0)
     cg::cluster_group cluster = cg::this_cluster();
     const int csize = static_cast<int>(cluster.num_blocks());
     const int crank = static_cast<int>(cluster.block_rank());
     const uint32_t total_slots = static_cast<uint32_t>(T) * static_cast<uint32_t>(csize);
-    const int threshold = static_cast<int>(0.8 * static_cast<double>(total_slots));
     const int rid = blockIdx.x / csize;
     const int row = p.rows[rid];
 
     for (int i = threadIdx.x; i < T; i += THREADS) smem[i] = kEmpty;
     if (threadIdx.x == 0) {
         s_count = 0;
-        s_abort = 0;
+        s_spill = 0;
+        s_total = 0;
     }
     cluster.sync();
 
-    int32_t* abort_flag = cluster.map_shared_rank(&s_abort, 0);
+    ClusterTableOps ops{cluster, smem, &s_count, &s_spill, &s_total, static_cast<uint32_t>(T),
+                        total_slots, static_cast<int32_t>(0.8 * static_cast<double>(total_slots)),
+                        csize};
     const int a0 = p.a_rpt[row];
     const int a1 = p.a_rpt[row + 1];
     // the cluster walks the row's A entries in slices of THREADS, CTA c taking
     // slices c, c + csize, ...
-    int local = 0;
     for (int base = a0 + crank * THREADS; base < a1; base += csize * THREADS) {
         const int end = min(base + THREADS, a1);
-        const bool stop = (*reinterpret_cast<volatile int32_t*>(abort_flag)) != 0;
-        if (__syncthreads_or(stop ? 1 : 0)) break;
+        if (__syncthreads_or(ops.spilled() ? 1 : 0)) break;
         cta_for_products<THREADS>(p.a_col, p.b_rpt, base, end, sc, [&](int qb, int) {
-            const int32_t key = __ldg(p.b_col + qb);
-            uint32_t h = hash_slot(key, total_slots);
-            for (uint32_t probe = 0; probe < total_slots; probe++) {
-                const int owner = static_cast<int>(h / T);
-                int32_t* slot = cluster.map_shared_rank(smem + (h % T), owner);
-                const int32_t old = atomicCAS(slot, kEmpty, key);
-                if (old == kEmpty) {
-                    local++;
-                    return;
-                }
-                if (old == key) return;
-                h = (h + 1 == total_slots) ? 0u : h + 1;
-            }
-            report(p.status, kStProbeLimit, row);
+            if (ops.spilled()) return;
+            cluster_insert(ops, __ldg(p.b_col + qb));
         });
-        // publish this slice's inserts; abort the row when the cluster table
-        // is past its load limit
-        const int slice = block_sum<THREADS>(local, sc.warp_tot);
-        local = 0;
-        if (threadIdx.x == 0) {
-            int32_t* cnt0 = cluster.map_shared_rank(&s_count, 0);
-            const int now = atomicAdd(cnt0, slice) + slice;
-            if (now > threshold) atomicExch(abort_flag, 1);
-        }
     }
     cluster.sync();
     if (crank == 0 && threadIdx.x == 0) {
-        if (s_abort != 0) {
+        if (s_spill != 0) {
             const int idx = atomicAdd(p.fail_count, 1);
             p.fail_rows[idx] = row;
             p.c_rpt[row] = 0;
         } else {
-            p.c_rpt[row] = s_count;
+            int total = 0;
+            for (int r = 0; r < csize; r++) total += *cluster.map_shared_rank(&s_count, r);
+            p.c_rpt[row] = total;
         }
     }
     cluster.sync();  // no CTA leaves while another may still touch its table

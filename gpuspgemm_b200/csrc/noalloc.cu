@@ -33,31 +33,44 @@ static __device__ __align__(256) uint32_t g_noalloc_bitmaps[kSlots * kWordsPerSl
 __global__ __launch_bounds__(kNoAllocThreads) void k_row_nnz_noalloc(
     const int32_t* __restrict__ a_rpt, const int32_t* __restrict__ a_col,
     const int32_t* __restrict__ b_rpt, const int32_t* __restrict__ b_col, int32_t m,
-    uint32_t* __restrict__ bitmaps, int32_t* __restrict__ nnz_out) {
+    int32_t n_cols, uint32_t* __restrict__ bitmaps, int32_t* __restrict__ nnz_out) {
     __shared__ CtaScratch<kNoAllocThreads> sc;
     uint32_t* bm = bitmaps + static_cast<size_t>(blockIdx.x) * kWordsPerSlot;
     for (int row = blockIdx.x; row < m; row += gridDim.x) {
         const int a0 = a_rpt[row];
         const int a1 = a_rpt[row + 1];
         int cnt = 0;
+        int bad = 0;
+        // a column outside [0, B.n) is skipped (it would index past this
+        // slot) and the row's count becomes -1
         cta_for_products<kNoAllocThreads>(a_col, b_rpt, a0, a1, sc, [&](int qb, int) {
             const int32_t key = __ldg(b_col + qb);
+            if (static_cast<uint32_t>(key) >= static_cast<uint32_t>(n_cols)) {
+                bad = 1;
+                return;
+            }
             const uint32_t bit = 1u << (key & 31);
             const uint32_t old = atomicOr(bm + (key >> 5), bit);
             cnt += (old & bit) ? 0 : 1;
         });
         cnt = block_sum<kNoAllocThreads>(cnt, sc.warp_tot);
-        if (threadIdx.x == 0) nnz_out[row] = cnt;
+        bad = __syncthreads_or(bad);
+        if (threadIdx.x == 0) nnz_out[row] = bad ? -1 : cnt;
+        // every thread has read the warp totals of block_sum before the next
+        // walk's scan writes them again
+        __syncthreads();
         // leave the slot all-zero for the next row: clear exactly the words
         // this row touched (several keys may share a word; zero is idempotent)
         cta_for_products<kNoAllocThreads>(a_col, b_rpt, a0, a1, sc, [&](int qb, int) {
-            bm[__ldg(b_col + qb) >> 5] = 0u;
+            const int32_t key = __ldg(b_col + qb);
+            if (static_cast<uint32_t>(key) < static_cast<uint32_t>(n_cols)) bm[key >> 5] = 0u;
         });
     }
 }
 
 std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[64] = {};  // device address of the slab, per device ordinal
+constexpr int kMaxDevices = 64;
+void* g_noalloc_ptr[kMaxDevices] = {};  // device address of the slab, per device ordinal
 
 }  // namespace
 
@@ -93,8 +106,13 @@ extern "C" spgemm_status spgemm_row_nnz_noalloc(const spgemm_csr_view* A,
         (A->nnz > 0 && A->col == nullptr) || (B->nnz > 0 && B->col == nullptr))
         return noalloc_fail(SPGEMM_ERR_INVALID_ARG, "NULL array");
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
-        return noalloc_fail(SPGEMM_ERR_CUDA, "cudaGetDevice failed");
+    if (cudaError_t e = cudaGetDevice(&dev); e != cudaSuccess)
+        return noalloc_fail(SPGEMM_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices)
+        return noalloc_fail(SPGEMM_ERR_UNSUPPORTED_DEVICE,
+                            "device ordinal " + std::to_string(dev) +
+                                " is beyond the allocation-free path's table of " +
+                                std::to_string(kMaxDevices) + " devices");
     void* slab = nullptr;
     {
         // once per device, with that device current: the host-side name of a
@@ -111,12 +129,17 @@ extern "C" spgemm_status spgemm_row_nnz_noalloc(const spgemm_csr_view* A,
         slab = g_noalloc_ptr[dev];
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    // the slab keeps whatever the last call left; it must start all-zero
-    cudaError_t e = cudaMemsetAsync(slab, 0, sizeof(uint32_t) * size_t(kSlots) * kWordsPerSlot, s);
+    // the slab keeps whatever the last call left; the words this call can
+    // touch (the first ceil(B.n / 32) of each slot in use) must start at zero
+    const int grid = A->m < kSlots ? A->m : kSlots;
+    const size_t words = (static_cast<size_t>(B->n) + 31) / 32;
+    cudaError_t e = cudaSuccess;
+    if (words > 0)
+        e = cudaMemset2DAsync(slab, sizeof(uint32_t) * kWordsPerSlot, 0, sizeof(uint32_t) * words,
+                              static_cast<size_t>(grid), s);
     if (e == cudaSuccess) {
-        const int grid = A->m < kSlots ? A->m : kSlots;
         k_row_nnz_noalloc<<<grid, kNoAllocThreads, 0, s>>>(A->rpt, A->col, B->rpt, B->col, A->m,
-                                                          static_cast<uint32_t*>(slab),
+                                                          B->n, static_cast<uint32_t*>(slab),
                                                           c_row_nnz);
         e = cudaGetLastError();
     }

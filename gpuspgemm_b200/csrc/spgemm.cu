@@ -1245,7 +1245,11 @@ spgemm_status product_host(spgemm_handle_s* h, const spgemm_csr_view* A,
                align_up(sizeof(int32_t) * size_t(v->nnz), 256) +
                align_up(sizeof(V) * size_t(v->nnz), 256);
     };
-    const size_t need = bytes_of(A) + bytes_of(B);
+    // C = A * A with one host matrix (the same arrays passed twice): copy it
+    // to the device once
+    const bool same = A->m == B->m && A->n == B->n && A->nnz == B->nnz && A->rpt == B->rpt &&
+                      A->col == B->col && A->val == B->val;
+    const size_t need = bytes_of(A) + (same ? 0 : bytes_of(B));
     if (spgemm_status st = regrow(h, &h->in_buf, &h->in_bytes, need, stream); st != SPGEMM_OK)
         return st;
     char* p = static_cast<char*>(h->in_buf);
@@ -1272,7 +1276,10 @@ spgemm_status product_host(spgemm_handle_s* h, const spgemm_csr_view* A,
     };
     spgemm_csr_view dA, dB;
     B200_TRY(upload(A, &dA));
-    B200_TRY(upload(B, &dB));
+    if (same)
+        dB = dA;
+    else
+        B200_TRY(upload(B, &dB));
     spgemm_csr_out dC;
     if (spgemm_status st = product<V>(h, &dA, &dB, &dC, stream); st != SPGEMM_OK) return st;
     std::memset(C, 0, sizeof(*C));

@@ -132,6 +132,7 @@ SPGEMM_API spgemm_status spgemm_csr_free(spgemm_csr_out* C, void* stream);
 /* C = A * B with HOST operands and a HOST result: copies A and B to the device,
  * multiplies, copies C back.  Replaces the apps' convert/run pair
  * (src/apps/proposal.cu:15-26: HostCSR::to<Device>, proposal, to<Host>).
+ * When A and B are the same host arrays (C = A * A), they are copied once.
  * C's three arrays live in one page-locked block from a process-wide pool
  * (so the device-to-host copy runs at full link speed); spgemm_host_csr_free
  * returns the block to the pool. */
@@ -377,8 +378,12 @@ SPGEMM_API spgemm_status spgemm_plan_destroy(spgemm_plan_t plan);
  *
  * Only the index arrays of A and B are read (val may be NULL).  B's columns
  * must lie in [0, B.n) with B.n <= SPGEMM_NOALLOC_MAX_COLS; larger B.n is
- * rejected with SPGEMM_ERR_INVALID_ARG.  Runs on the current device and
- * returns without synchronising (stream-ordered on `stream`).
+ * rejected with SPGEMM_ERR_INVALID_ARG.  A column of B outside [0, B.n) is
+ * skipped, and every row of C that reaches it gets the count -1 (the call
+ * itself does not synchronise, so the check is reported in the output).
+ * Runs on the current device and returns without synchronising
+ * (stream-ordered on `stream`).  At most 32 CTAs run (one per scratch slot),
+ * so large products take longer here than in spgemm_csr_*.
  *
  * Scratch: a fixed 4 MiB bitmap area compiled into the library's device image
  * (every GPU that loads the library holds it until the process exits).  The

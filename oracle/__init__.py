@@ -25,7 +25,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libref_proposal.so"
-REF_SRC = Path("/root/reference/src")
+# root of the reference checkout (read-only), from the environment when set
+REF_ROOT = Path(os.environ.get("GPUSPGEMM_REFERENCE", "/root/reference"))
+REF_SRC = REF_ROOT / "src"
 
 sys.path.insert(0, str(HERE.parent))
 from gpuspgemm_b200.csr import HostCSR  # noqa: E402
@@ -40,7 +42,7 @@ def build(ref: bool | None = None) -> None:
         ref = REF_SRC.exists()
     if ref:
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", "opsparse",
-                        f"PYTHON={sys.executable}"], check=True)
+                        f"PYTHON={sys.executable}", f"REF_SRC={REF_SRC}"], check=True)
 
 
 _lib = None

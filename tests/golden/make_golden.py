@@ -98,4 +98,6 @@ def main(outdir: str) -> int:
 
 
 if __name__ == "__main__":
-    sys.exit(main(sys.argv[1] if len(sys.argv) > 1 else "gpurun_out/golden"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py OUTPUT_DIR")
+    sys.exit(main(sys.argv[1]))

@@ -51,8 +51,9 @@ def check(oracle, A, B, C, dtype, name, positive=False):
 @pytest.fixture(scope="module", autouse=True)
 def _dump_results():
     yield
-    out = Path(os.environ.get("SPGEMM_PARITY_OUT", "gpurun_out"))
-    if out.is_dir():
+    # the per-case error figures, when SPGEMM_PARITY_OUT names a folder
+    out = Path(os.environ.get("SPGEMM_PARITY_OUT", "")) if os.environ.get("SPGEMM_PARITY_OUT") else None
+    if out is not None and out.is_dir():
         (out / "parity_results.json").write_text(json.dumps(RESULTS, indent=1, default=str))
 
 
@@ -391,6 +392,32 @@ def test_heavy_row_spills_to_global(handle, oracle_mod):
         handle.set_option(N.OPT_ONE_PASS, 0)
     check(oracle_mod, A, B, C, np.float64, "heavy_row_spill", positive=False)
     assert info["max_row_nnz"] > 150_000
+
+
+def test_row_past_the_cluster_table_spills(handle, oracle_mod):
+    """A row with more distinct columns (230,400) than the cluster count
+    table's 4 x 55,296 slots: the insert loop's load test spills it to the
+    global bitmap bin as soon as the table passes its limit, and the fill
+    runs in the global bin of the wide ladder (B.n > 2^20).  Its A entries
+    span five slices of 1,024, so each slice adds at most 46,080 keys."""
+    n_a, per = 5 * 1024, 45
+    b_col = np.arange(n_a * per, dtype=np.int32)       # B row j: columns j*45 .. j*45+44
+    rng = np.random.default_rng(61)
+    B = HostCSR(n_a, (1 << 21) + 7, np.arange(0, n_a * per + 1, per, dtype=np.int32), b_col,
+                rng.uniform(0.1, 1.0, n_a * per))
+    A = HostCSR(2, n_a, np.array([0, n_a, n_a + 3], np.int32),
+                np.concatenate([np.arange(n_a, dtype=np.int32), np.array([2, 7, 11], np.int32)]),
+                rng.uniform(0.1, 1.0, n_a + 3))
+    from gpuspgemm_b200 import _native as N
+    handle.set_option(N.OPT_ONE_PASS, 2)  # the count phase: cluster table, then its spill
+    try:
+        C = gpu_product(A, B, handle, np.float64)
+        info = handle.info()
+    finally:
+        handle.set_option(N.OPT_ONE_PASS, 0)
+    check(oracle_mod, A, B, C, np.float64, "row_past_cluster_table", positive=True)
+    assert info["max_row_nnz"] == n_a * per
+    assert info["sym_fail_rows"] >= 1
 
 
 def test_edge_cases(handle, oracle_mod):

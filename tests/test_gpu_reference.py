@@ -6,8 +6,8 @@ reference sources for sm_100a (`make -C oracle ref`).  These tests need that
 build; they are skipped where it is absent.  Besides parity they time both
 implementations the way the reference's `measure` lambda does (wall clock
 around the call plus a device synchronize, C allocated and freed inside;
-src/apps/proposal.cu:28-35) and write the figures to
-gpurun_out/ref_compare.json.
+src/apps/proposal.cu:28-35) and, when SPGEMM_PARITY_OUT names a folder, write
+the figures to ref_compare.json there.
 """
 import json
 import os
@@ -21,14 +21,14 @@ from gpuspgemm_b200 import generators as G
 
 pytestmark = pytest.mark.gpu
 
-OUT = Path(os.environ.get("SPGEMM_PARITY_OUT", "gpurun_out"))
+OUT = Path(os.environ["SPGEMM_PARITY_OUT"]) if os.environ.get("SPGEMM_PARITY_OUT") else None
 RECORDS = {}
 
 
 @pytest.fixture(scope="module", autouse=True)
 def _dump():
     yield
-    if OUT.is_dir() and RECORDS:
+    if OUT is not None and OUT.is_dir() and RECORDS:
         (OUT / "ref_compare.json").write_text(json.dumps(RECORDS, indent=1))
 
 
@@ -56,7 +56,18 @@ CASES = {
     "uniform4096x8_f64": (lambda: G.uniform_rows(4096, 8), np.float64),
     "powerlaw1M_f64": (lambda: G.power_law(), np.float64),
     "powerlaw1M_f32": (lambda: G.power_law(), np.float32),
+    # the power-law matrix at ~3.1 M nnz (Zipf exponent 2.2)
+    "powerlaw1M_zipf2.2_f64": (lambda: G.power_law(1_000_000, 2.2, 4700), np.float64),
 }
+
+
+def _reference_equal(C, R):
+    """The reference's operator== (csr.cuh:218-239): same structure, every
+    value within 1e-8 + 1e-5 * max(|l|, |r|)."""
+    if not (np.array_equal(C.rpt, R.rpt) and np.array_equal(C.col, R.col)):
+        return False
+    l, r = C.val.astype(np.float64), R.val.astype(np.float64)
+    return bool(np.all(np.abs(l - r) <= 1e-8 + 1e-5 * np.maximum(np.abs(l), np.abs(r))))
 
 
 @pytest.mark.parametrize("name", list(CASES))
@@ -80,6 +91,22 @@ def test_against_reference_build(handle, oracle_mod, name):
            "ours_s": ts, "reference_proposal_s": ref_ts,
            "ours_gflops_median": 2 * nip / float(np.median(ts)) / 1e9,
            "reference_gflops_median": 2 * nip / float(np.median(ref_ts)) / 1e9}
+    # the reference's validate path (cuSPARSE SpGEMM ALG2, common.hpp:109-126):
+    # identical structure, values within its own tolerance
+    CS = oracle_mod.ref_cusparse2(A, A, dt)
+    assert np.array_equal(C.rpt, CS.rpt), "row pointers differ from cuSPARSE ALG2"
+    assert np.array_equal(C.col, CS.col), "column indices differ from cuSPARSE ALG2"
+    assert _reference_equal(C, CS)
+    # each sums the products in its own order: compare against the
+    # cancellation-aware bound sum_k |a_ik||b_kj| (the relative error where
+    # the values cannot cancel)
+    A64 = A.astype(np.float64)
+    bound = oracle_mod.abs_bound(A64, A64, CS)
+    diff = np.abs(C.val.astype(np.float64) - CS.val.astype(np.float64))
+    max_cond_cs = float((diff / np.where(bound > 0, bound, 1.0)).max()) if CS.nnz else 0.0
+    assert max_cond_cs <= tol, max_cond_cs
+    rec["max_err_over_bound_vs_cusparse2"] = max_cond_cs
+    del CS
     try:
         cs_ts, _ = oracle_mod.ref_time("cusparse2", A, A, dt, warmups=1, runs=3)
         rec["cusparse2_s"] = cs_ts

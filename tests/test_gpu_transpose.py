@@ -129,6 +129,25 @@ def test_galerkin_rap(handle, oracle_mod, given_r, dtype):
     assert info["nip"] == oracle_mod.nip(A, P) + oracle_mod.nip(R, oracle_mod.spgemm(A, P))
 
 
+def test_galerkin_rap_stencil100(handle, oracle_mod):
+    """The Galerkin workload at its stated size: 27-point stencil on 100^3
+    (1e6 rows, 26.5 M nnz), aggregation prolongator P (1e6 x 35,937), R = P^T
+    on the device; R * (A * P) against the oracle chain."""
+    from gpuspgemm_b200.api import DeviceCSR, rap
+    A = G.stencil27(100)
+    P = G.aggregation_prolongator(100, seed=5)
+    assert A.nnz == 298 ** 3
+    dA, dP = DeviceCSR.from_host(A), DeviceCSR.from_host(P)
+    C = rap(dA, dP, None, handle).to_host()
+    del dA, dP
+    R = oracle_mod.transpose(P)
+    ref, bound = _chain_reference(oracle_mod, R, A, P)
+    assert (C.m, C.n) == (P.n, P.n)
+    assert np.array_equal(C.rpt, ref.rpt) and np.array_equal(C.col, ref.col)
+    err = np.abs(C.val - ref.val) / bound.val
+    assert float(err.max()) <= 1e-12, float(err.max())
+
+
 def test_rap_dimension_checks(handle):
     from gpuspgemm_b200 import SpgemmError
     from gpuspgemm_b200.api import DeviceCSR, rap
