@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--grid", type=int, default=100,
                     help="galerkin mode: points per dimension of the 27-point stencil")
     ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--streams", type=int, default=None,
+                    help="plain mode: side streams of the handle (default: the library's)")
     ap.add_argument("--no-tune", action="store_true",
                     help="batch mode: plan the batch without the autotuner")
     ap.add_argument("--requests", type=int, default=600)
@@ -319,6 +321,8 @@ def run_ours(args, rank, world, local_rank):
     A = workload(args)
     dA = DeviceCSR.from_host(A, dev)
     h = Handle(local_rank)
+    if args.streams is not None:
+        h.set_option(N.OPT_STREAMS, args.streams)
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
@@ -516,6 +520,7 @@ def run_ours(args, rank, world, local_rank):
         "kernels": kernels[:12],
         "serial_kernel_ms_per_step": serial_total,
         "host_syncs_per_step": info["host_syncs"],
+        "side_streams": nside,
         "host_phase_us_last_step": phase_us,
         "plan_replay": {"ms": plan_replay_ms, "gflops": 2.0 * nip / (plan_replay_ms / 1e3) / 1e9,
                         "what": "fill phase only, structure fixed: one CUDA graph launch "
@@ -741,6 +746,9 @@ def served_pool(seed: int):
     return [[DeviceCSR.from_host(a) for a in pool] for pool in (small, medium, large)]
 
 
+SERVER_WORKERS = 2
+
+
 def run_served(args, local_rank):
     import time as _t
 
@@ -785,8 +793,7 @@ def run_served(args, local_rank):
         return np.array(lat), _t.perf_counter() - t_start
 
     def served(arrivals):
-        server = SpgemmServer(memory_budget=48 << 30, max_batch=256, workers=2,
-                              device=local_rank)
+        server = SpgemmServer(memory_budget=48 << 30, workers=SERVER_WORKERS, device=local_rank)
         reqs = []
         t_start = _t.perf_counter()
         for d, ta in zip(picks, arrivals):
@@ -844,7 +851,8 @@ def run_served(args, local_rank):
                 "<=256k rows, 5% the 1M power-law",
         "config": {"requests": len(picks), "mix": {k: int((kinds == i).sum()) for i, k in
                                                    enumerate(["small", "medium", "large"])},
-                   "nip_total": total_nip, "memory_budget_bytes": 48 << 30, "workers": 2},
+                   "nip_total": total_nip, "memory_budget_bytes": 48 << 30,
+                   "workers": SERVER_WORKERS},
         "saturation": {"served_products_per_s": len(picks) / span_sat,
                        "plain_products_per_s": len(picks) / span_plain_sat,
                        "speedup": span_plain_sat / span_sat,

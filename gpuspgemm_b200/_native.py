@@ -22,7 +22,7 @@ STATUS_NAMES = {
     7: "SPGEMM_ERR_INTERNAL",
 }
 
-ABI_VERSION = 4  # SPGEMM_ABI_VERSION of include/spgemm.h
+ABI_VERSION = 5  # SPGEMM_ABI_VERSION of include/spgemm.h
 
 OPT_CHECKED = 1
 OPT_MIN_SYM_BIN = 2
@@ -75,13 +75,17 @@ class Info(C.Structure):
     ]
 
 
+PLAN_MAX_CANDIDATES = 16  # SPGEMM_PLAN_MAX_CANDIDATES
+
+
 class PlanInfo(C.Structure):
     _fields_ = [
         ("candidates", C.c_int32),
         ("chosen", C.c_int32),
-        ("team_scale", C.c_float * 8),
-        ("streams", C.c_int32 * 8),
-        ("ms", C.c_float * 8),
+        ("team_scale", C.c_float * PLAN_MAX_CANDIDATES),
+        ("cta_scale", C.c_float * PLAN_MAX_CANDIDATES),
+        ("streams", C.c_int32 * PLAN_MAX_CANDIDATES),
+        ("ms", C.c_float * PLAN_MAX_CANDIDATES),
     ]
 
 

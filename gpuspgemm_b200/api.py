@@ -359,6 +359,7 @@ class Plan:
         N.check(N.lib().spgemm_plan_get_info(self._p, C.byref(inf)))
         n = int(inf.candidates)
         return {"candidates": [{"team_scale": round(float(inf.team_scale[i]), 3),
+                                "cta_scale": round(float(inf.cta_scale[i]), 3),
                                 "streams": int(inf.streams[i]), "ms": float(inf.ms[i])}
                                for i in range(n)],
                 "chosen": int(inf.chosen)}

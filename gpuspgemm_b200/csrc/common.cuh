@@ -141,6 +141,84 @@ __device__ __forceinline__ void team_for_products_at(const int32_t* __restrict__
     }
 }
 
+// The same walk with up to U products per lane in flight: a lane takes
+// products q, q + G, ..., q + (U-1) G of the chunk together, runs their
+// shuffle searches interleaved, issues every `load(q_b, a_index, q_row)` (the
+// product's global reads, returning a value), then every
+// `use(value, q_b, a_index, q_row)`.  Same products, same arguments as
+// team_for_products_at.
+//
+// With CONVERGED set every lane of the team calls
+// `use(value, q_b, a_index, q_row, valid)` together, valid telling whether the
+// lane holds a product, so `use` may contain operations on the team's mask.
+template<int G, int U, bool CONVERGED = false, typename L, typename F>
+__device__ __forceinline__ void team_for_products_mlp(const int32_t* __restrict__ a_col,
+                                                      const int32_t* __restrict__ b_rpt, int a0,
+                                                      int a1, L&& load, F&& use) {
+    if constexpr (U == 1 && !CONVERGED) {
+        // one product per lane: the plain walk (fewer registers)
+        team_for_products_at<G>(a_col, b_rpt, a0, a1,
+                                [&](int qb, int ai, int q) { use(load(qb, ai, q), qb, ai, q); });
+        return;
+    }
+    using Val = decltype(load(0, 0, 0));
+    const unsigned mask = team_mask<G>();
+    const int lane = team_lane<G>();
+    int off = 0;
+    for (int base = a0; base < a1; base += G) {
+        const int e = base + lane;
+        int bs = 0;
+        int len = 0;
+        if (e < a1) {
+            const int c = __ldg(a_col + e);
+            bs = __ldg(b_rpt + c);
+            len = __ldg(b_rpt + c + 1) - bs;
+        }
+        const int inc = team_inclusive_scan<G>(mask, len, lane);
+        const int total = __shfl_sync(mask, inc, G - 1, G);
+        const int exc = inc - len;
+        for (int q0 = 0; q0 < total; q0 += G * U) {
+            // steps of this round that hold products (uniform over the team)
+            const int nu = min(U, (total - q0 + G - 1) / G);
+            int s[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) s[u] = 0;
+#pragma unroll
+            for (int step = G / 2; step > 0; step >>= 1) {
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    if (u < nu) {
+                        const int cand = __shfl_sync(mask, exc, s[u] + step, G);
+                        if (cand <= q0 + u * G + lane) s[u] += step;
+                    }
+                }
+            }
+            Val v[U];
+            int qb[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (u < nu) {
+                    const int q = q0 + u * G + lane;
+                    const int sbs = __shfl_sync(mask, bs, s[u], G);
+                    const int sexc = __shfl_sync(mask, exc, s[u], G);
+                    qb[u] = sbs + q - sexc;
+                    if (q < total) v[u] = load(qb[u], base + s[u], off + q);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int q = q0 + u * G + lane;
+                if constexpr (CONVERGED) {
+                    if (u < nu) use(v[u], qb[u], base + s[u], off + q, q < total);
+                } else {
+                    if (u < nu && q < total) use(v[u], qb[u], base + s[u], off + q);
+                }
+            }
+        }
+        off += total;
+    }
+}
+
 // The same walk for callers that need no product position: f(q_b, a_index).
 template<int G, typename F>
 __device__ __forceinline__ void team_for_products(const int32_t* __restrict__ a_col,
@@ -163,6 +241,16 @@ __device__ __forceinline__ int lower_bound_present(const int32_t* cols, int n, i
     return lo;
 }
 
+// Warp-cooperative insert: the lanes of `mask` (converged, every one calling)
+// that hold the same key elect their lowest lane, and only that lane probes
+// the table, so a key repeated across the lanes costs one CAS sequence
+// instead of one per lane contending for the same slot.  Lanes with `valid`
+// false take part in the match only.  Returns 1 on the electing lane when the
+// key was new, else 0 -- the lanes' sum is the number of new keys.
+__device__ __forceinline__ int table_insert_dedup(int32_t* table, uint32_t T, int32_t key,
+                                                  bool valid, unsigned mask, DevStatus* st,
+                                                  int32_t row);
+
 // Insert `key` into a linear-probing table of T slots.  Returns 1 if the key
 // was new, 0 if already present.  The probe loop is bounded by T; if it runs
 // out (table full -- impossible for rows routed by their bound) the status
@@ -178,6 +266,15 @@ __device__ __forceinline__ int table_insert(int32_t* table, uint32_t T, int32_t 
     }
     report(st, kStProbeLimit, row);
     return 0;
+}
+
+__device__ __forceinline__ int table_insert_dedup(int32_t* table, uint32_t T, int32_t key,
+                                                  bool valid, unsigned mask, DevStatus* st,
+                                                  int32_t row) {
+    // kEmpty is never a column index, so lanes without a product group apart
+    const unsigned peers = __match_any_sync(mask, valid ? key : kEmpty);
+    const bool leader = (threadIdx.x & 31u) == static_cast<unsigned>(__ffs(peers) - 1);
+    return (valid && leader) ? table_insert(table, T, key, st, row) : 0;
 }
 
 }  // namespace b200

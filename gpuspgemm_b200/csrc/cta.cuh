@@ -107,6 +107,80 @@ __device__ __forceinline__ void cta_for_products_at(const int32_t* __restrict__ 
     }
 }
 
+// The same walk with U products per thread in flight: each thread takes
+// products q, q + THREADS, ..., q + (U-1) THREADS together, runs their U
+// binary searches interleaved (one shared trip count), issues every
+// `load(q_b, a_index, q_row)` -- the product's global reads, returning a value
+// -- and only then every `use(value, q_b, a_index, q_row)`.  A walk whose
+// work is a dependent global read followed by a shared-memory update thus
+// keeps U reads outstanding per thread instead of one.  Same products, same
+// arguments as cta_for_products_at.
+//
+// With CONVERGED set, whole warps take products together (lane l of a warp
+// takes the warp's base + l) and every lane calls
+// `use(value, q_b, a_index, q_row, valid)`, valid telling whether the lane holds
+// a product, so `use` may contain warp-wide operations on the full mask.
+template<int THREADS, int U, bool CONVERGED = false, typename L, typename F>
+__device__ __forceinline__ void cta_for_products_mlp(const int32_t* __restrict__ a_col,
+                                                     const int32_t* __restrict__ b_rpt, int a0,
+                                                     int a1, CtaScratch<THREADS>& sc, L&& load,
+                                                     F&& use) {
+    using Val = decltype(load(0, 0, 0));
+    const int tid = threadIdx.x;
+    int off = 0;
+    for (int base = a0; base < a1; base += THREADS) {
+        const int e = base + tid;
+        int bs = 0;
+        int len = 0;
+        if (e < a1) {
+            const int c = __ldg(a_col + e);
+            bs = __ldg(b_rpt + c);
+            len = __ldg(b_rpt + c + 1) - bs;
+        }
+        const int inc = block_inclusive_scan<THREADS>(len, sc.warp_tot);
+        sc.exc[tid] = inc - len;
+        sc.bs[tid] = bs;
+        if (tid == THREADS - 1) sc.total = inc;
+        __syncthreads();
+        const int total = sc.total;
+        const int nvalid = min(THREADS, a1 - base);
+        // CONVERGED: the loop bound is the warp's first lane's, so a warp
+        // enters and leaves together
+        const int tid0 = CONVERGED ? (tid & ~(kWarp - 1)) : tid;
+        for (int q0 = tid, w0 = tid0; w0 < total; q0 += THREADS * U, w0 += THREADS * U) {
+            int lo[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) lo[u] = 0;
+            for (int n = nvalid; n > 1;) {
+                const int half = n >> 1;
+#pragma unroll
+                for (int u = 0; u < U; u++)
+                    lo[u] = (sc.exc[lo[u] + half] <= q0 + u * THREADS) ? lo[u] + half : lo[u];
+                n -= half;
+            }
+            Val v[U];
+            int qb[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int q = q0 + u * THREADS;
+                qb[u] = sc.bs[lo[u]] + q - sc.exc[lo[u]];
+                if (q < total) v[u] = load(qb[u], base + lo[u], off + q);
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int q = q0 + u * THREADS;
+                if constexpr (CONVERGED) {
+                    use(v[u], qb[u], base + lo[u], off + q, q < total);
+                } else {
+                    if (q < total) use(v[u], qb[u], base + lo[u], off + q);
+                }
+            }
+        }
+        off += total;
+        __syncthreads();
+    }
+}
+
 // The same walk for callers that need no product position: f(q_b, a_index).
 template<int THREADS, typename F>
 __device__ __forceinline__ void cta_for_products(const int32_t* __restrict__ a_col,

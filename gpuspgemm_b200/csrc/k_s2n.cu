@@ -30,6 +30,26 @@ __device__ __forceinline__ V ldv(const void* base, int i) {
     return __ldg(static_cast<const V*>(base) + i);
 }
 
+// What a fill walk loads for one product: B's column and the rounded product
+// a_ik * b_kj.  The walks keep kWalkU products per thread in flight.
+template<typename V>
+struct KeyProduct {
+    int32_t key;
+    V prod;
+};
+// Products in flight per thread, per walk (measured on the 1M power-law
+// product, serialised per-kernel times): the CTA walks 4 (the 256-thread
+// expand-sort-compress bin 0.285 -> 0.261 ms), the bitmap bin 2 (0.470 ->
+// 0.449 ms; 4 gave 0.456), the 16- and 32-lane teams 2 (0.140 -> 0.124 ms for
+// 32 lanes), the 4- and 8-lane teams 1 (their rows hold few products; 2 and
+// 4 cost registers and took 0.097 -> 0.114 / 0.124 ms for 4 lanes).
+constexpr int kWalkU = 4;
+constexpr int kBitmapWalkU = 2;
+template<int G>
+constexpr int team_walk_u() {
+    return G >= 16 ? 2 : 1;
+}
+
 // Values accumulate straight into the row's slice of C.val with global
 // reductions (fire-and-forget FP64 adds in L2; the row's slice was zeroed by
 // the same team or CTA before the barrier that precedes them).  That keeps no
@@ -59,9 +79,11 @@ __global__ __launch_bounds__(THREADS) void k_s2n_team(ProductArgs p) {
     team_sync<G>(mask);
     const int a0 = p.a_rpt[row];
     const int a1 = p.a_rpt[row + 1];
-    team_for_products<G>(p.a_col, p.b_rpt, a0, a1, [&](int qb, int) {
-        table_insert(keys, T, __ldg(p.b_col + qb), p.status, row);
-    });
+    team_for_products_mlp<G, team_walk_u<G>(), true>(
+        p.a_col, p.b_rpt, a0, a1, [&](int qb, int, int) { return __ldg(p.b_col + qb); },
+        [&](int32_t key, int, int, int, bool valid) {
+            table_insert_dedup(keys, T, key, valid, mask, p.status, row);
+        });
     team_sync<G>(mask);
     // sort only the row's keys: compact them to the front, then the register
     // sort leaves them in swizzled order (sort.cuh)
@@ -80,11 +102,14 @@ __global__ __launch_bounds__(THREADS) void k_s2n_team(ProductArgs p) {
         out[i] = V(0);
     }
     team_sync<G>(mask);
-    team_for_products<G>(p.a_col, p.b_rpt, a0, a1, [&](int qb, int ai) {
-        const int32_t key = __ldg(p.b_col + qb);
-        const int pos = lower_bound_present_swz(keys, nnz, key);
-        atomicAdd(out + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
-    });
+    team_for_products_mlp<G, team_walk_u<G>()>(
+        p.a_col, p.b_rpt, a0, a1,
+        [&](int qb, int ai, int) {
+            return KeyProduct<V>{__ldg(p.b_col + qb), ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb)};
+        },
+        [&](const KeyProduct<V>& kp, int, int, int) {
+            atomicAdd(out + lower_bound_present_swz(keys, nnz, kp.key), kp.prod);
+        });
 }
 
 // Expand-sort-compress fill of rows with at most NMAX products, for the
@@ -130,22 +155,24 @@ __global__ __launch_bounds__(THREADS) void k_esc_team(ProductArgs p) {
         if (lane == 0) report(p.status, kStCapacity, row, nip);
         return;
     }
-    team_for_products_at<G>(p.a_col, p.b_rpt, p.a_rpt[row], p.a_rpt[row + 1],
-                            [&](int qb, int ai, int q) {
-                                if (q < NMAX) {
-                                    int32_t col = __ldg(p.b_col + qb);
-                                    // a column outside [0, B.n) would corrupt
-                                    // the packed key: report it, keep the key
-                                    // in range
-                                    if (static_cast<uint32_t>(col) >=
-                                        static_cast<uint32_t>(p.n_cols)) {
-                                        report(p.status, kStBadInput, row, col);
-                                        col = 0;
-                                    }
-                                    keys[q] = (col << SHIFT) | q;
-                                    vals[q] = ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb);
-                                }
-                            });
+    team_for_products_mlp<G, team_walk_u<G>()>(
+        p.a_col, p.b_rpt, p.a_rpt[row], p.a_rpt[row + 1],
+        [&](int qb, int ai, int) {
+            return KeyProduct<V>{__ldg(p.b_col + qb), ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb)};
+        },
+        [&](const KeyProduct<V>& kp, int, int, int q) {
+            if (q < NMAX) {
+                int32_t col = kp.key;
+                // a column outside [0, B.n) would corrupt the packed key:
+                // report it, keep the key in range
+                if (static_cast<uint32_t>(col) >= static_cast<uint32_t>(p.n_cols)) {
+                    report(p.status, kStBadInput, row, col);
+                    col = 0;
+                }
+                keys[q] = (col << SHIFT) | q;
+                vals[q] = kp.prod;
+            }
+        });
     team_sync<G>(mask);
     team_sort_swz<G, T / G>(keys, nip, mask, lane);
     int32_t* out_col = p.c_col + c0;
@@ -216,20 +243,22 @@ __global__ __launch_bounds__(THREADS) void k_esc_cta(ProductArgs p) {
         if (tid == 0) report(p.status, kStCapacity, row, nip);
         return;
     }
-    cta_for_products_at<THREADS>(p.a_col, p.b_rpt, p.a_rpt[row], p.a_rpt[row + 1], sc,
-                                 [&](int qb, int ai, int q) {
-                                     if (q >= NMAX) return;
-                                     int32_t col = __ldg(p.b_col + qb);
-                                     if (static_cast<uint32_t>(col) >=
-                                         static_cast<uint32_t>(p.n_cols)) {
-                                         report(p.status, kStBadInput, row, col);
-                                         col = 0;
-                                     }
-                                     const uint32_t u =
-                                         (static_cast<uint32_t>(col) << SHIFT) | static_cast<uint32_t>(q);
-                                     keys[q] = static_cast<int32_t>(u ^ 0x80000000u);
-                                     vals[q] = ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb);
-                                 });
+    cta_for_products_mlp<THREADS, kWalkU>(
+        p.a_col, p.b_rpt, p.a_rpt[row], p.a_rpt[row + 1], sc,
+        [&](int qb, int ai, int) {
+            return KeyProduct<V>{__ldg(p.b_col + qb), ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb)};
+        },
+        [&](const KeyProduct<V>& kp, int, int, int q) {
+            if (q >= NMAX) return;
+            int32_t col = kp.key;
+            if (static_cast<uint32_t>(col) >= static_cast<uint32_t>(p.n_cols)) {
+                report(p.status, kStBadInput, row, col);
+                col = 0;
+            }
+            const uint32_t u = (static_cast<uint32_t>(col) << SHIFT) | static_cast<uint32_t>(q);
+            keys[q] = static_cast<int32_t>(u ^ 0x80000000u);
+            vals[q] = kp.prod;
+        });
     cta_sort_swz<THREADS>(keys, nip);
     auto unkey = [&](int i) { return static_cast<uint32_t>(keys[swz(i)]) ^ 0x80000000u; };
     const int per = (nip + THREADS - 1) / THREADS;
@@ -390,9 +419,11 @@ __global__ __launch_bounds__(THREADS) void k_s2n_cta(ProductArgs p) {
     __syncthreads();
     const int a0 = p.a_rpt[row];
     const int a1 = p.a_rpt[row + 1];
-    cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int) {
-        table_insert(keys, T, __ldg(p.b_col + qb), p.status, row);
-    });
+    cta_for_products_mlp<THREADS, kWalkU, true>(
+        p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int, int) { return __ldg(p.b_col + qb); },
+        [&](int32_t key, int, int, int, bool valid) {
+            table_insert_dedup(keys, T, key, valid, 0xffffffffu, p.status, row);
+        });
     const int cnt = cta_compact<THREADS>(keys, T, sc.warp_tot);
     int nnz = bound;
     if (p.row_nnz != nullptr) {  // one-pass: the count is the row's nnz
@@ -412,11 +443,14 @@ __global__ __launch_bounds__(THREADS) void k_s2n_cta(ProductArgs p) {
         out[i] = V(0);
     }
     __syncthreads();
-    cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int ai) {
-        const int32_t key = __ldg(p.b_col + qb);
-        const int pos = lower_bound_present_swz(keys, nnz, key);
-        atomicAdd(out + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
-    });
+    cta_for_products_mlp<THREADS, kWalkU>(
+        p.a_col, p.b_rpt, a0, a1, sc,
+        [&](int qb, int ai, int) {
+            return KeyProduct<V>{__ldg(p.b_col + qb), ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb)};
+        },
+        [&](const KeyProduct<V>& kp, int, int, int) {
+            atomicAdd(out + lower_bound_present_swz(keys, nnz, kp.key), kp.prod);
+        });
 }
 
 // Bitmap bin (B.n <= kBitmapCols): the row's hash table is the identity hash
@@ -467,11 +501,18 @@ __global__ __launch_bounds__(THREADS) void k_s2n_bitmap(ProductArgs p) {
         if (tid == 0 && blockIdx.x < p.nrows) report(p.status, kStCapacity, p.rows[blockIdx.x], 0);
         return;
     }
+    __shared__ int32_t s_rid;  // the row this CTA takes next
     for (int i = tid; i < words; i += THREADS) bm[i] = 0u;
     summary[tid] = 0u;
-    __syncthreads();
     const int w0 = tid * 32;  // this thread's bitmap words [w0, w0 + 32)
-    for (int rid = blockIdx.x; rid < p.nrows; rid += gridDim.x) {
+    for (int k = 0;; k++) {
+        // rows are taken from the launch's counter as CTAs free up (the list
+        // is ordered largest first), so the CTAs finish together
+        __syncthreads();
+        if (tid == 0) s_rid = p.work != nullptr ? atomicAdd(p.work, 1) : blockIdx.x + k * gridDim.x;
+        __syncthreads();
+        const int rid = s_rid;
+        if (rid >= p.nrows) break;
         const int row = p.rows[rid];
         const int c0 = p.c_rpt[row];
         // the row's exact nnz, or in one-pass mode its NIP (an upper bound)
@@ -482,16 +523,17 @@ __global__ __launch_bounds__(THREADS) void k_s2n_bitmap(ProductArgs p) {
         }
         const int a0 = p.a_rpt[row];
         const int a1 = p.a_rpt[row + 1];
-        cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int) {
-            const int32_t key = __ldg(p.b_col + qb);
-            if (static_cast<uint32_t>(key) >= static_cast<uint32_t>(p.n_cols)) {
-                report(p.status, kStBadInput, row, key);  // outside the bitmap
-                return;
-            }
-            const int wi = key >> 5;
-            if (atomicOr(bm + wi, 1u << (key & 31)) == 0u)
-                atomicOr(summary + (wi >> 5), 1u << (wi & 31));
-        });
+        cta_for_products_mlp<THREADS, kBitmapWalkU>(
+            p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int, int) { return __ldg(p.b_col + qb); },
+            [&](int32_t key, int, int, int) {
+                if (static_cast<uint32_t>(key) >= static_cast<uint32_t>(p.n_cols)) {
+                    report(p.status, kStBadInput, row, key);  // outside the bitmap
+                    return;
+                }
+                const int wi = key >> 5;
+                if (atomicOr(bm + wi, 1u << (key & 31)) == 0u)
+                    atomicOr(summary + (wi >> 5), 1u << (wi & 31));
+            });
         const uint32_t sw = summary[tid];
         int cnt = 0;
         for (uint32_t m = sw; m != 0u; m &= m - 1u) cnt += __popc(bm[w0 + __ffs(m) - 1]);
@@ -520,20 +562,169 @@ __global__ __launch_bounds__(THREADS) void k_s2n_bitmap(ProductArgs p) {
         V* out = static_cast<V*>(p.c_val) + c0;
         for (int i = tid; i < nnz; i += THREADS) out[i] = V(0);
         __syncthreads();
-        cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int ai) {
-            const int32_t key = __ldg(p.b_col + qb);
-            if (static_cast<uint32_t>(key) >= static_cast<uint32_t>(p.n_cols)) return;
-            const int wi = key >> 5;
-            const int w8 = wi & ~7;
-            int rank = block_rank[wi >> 3] + __popc(bm[wi] & ((1u << (key & 31)) - 1u));
+        cta_for_products_mlp<THREADS, kBitmapWalkU>(
+            p.a_col, p.b_rpt, a0, a1, sc,
+            [&](int qb, int ai, int) {
+                return KeyProduct<V>{__ldg(p.b_col + qb), ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb)};
+            },
+            [&](const KeyProduct<V>& kp, int, int, int) {
+                const int32_t key = kp.key;
+                if (static_cast<uint32_t>(key) >= static_cast<uint32_t>(p.n_cols)) return;
+                const int wi = key >> 5;
+                const int w8 = wi & ~7;
+                int rank = block_rank[wi >> 3] + __popc(bm[wi] & ((1u << (key & 31)) - 1u));
 #pragma unroll
-            for (int t = 0; t < 7; t++)
-                if (w8 + t < wi) rank += __popc(bm[w8 + t]);
-            if (rank < nnz) atomicAdd(out + rank, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
-        });
+                for (int t = 0; t < 7; t++)
+                    if (w8 + t < wi) rank += __popc(bm[w8 + t]);
+                if (rank < nnz) atomicAdd(out + rank, kp.prod);
+            });
         for (uint32_t m = sw; m != 0u; m &= m - 1u) bm[w0 + __ffs(m) - 1] = 0u;
         summary[tid] = 0u;
         __syncthreads();
+    }
+}
+
+// Cluster bitmap bin (wide B, 2^20 < B.n <= kClusterBitmapCols): the
+// bitmap bin's bitmap, summary and block ranks spread over a thread-block
+// cluster -- CTA c of the cluster holds columns [c 2^20, (c + 1) 2^20) in its
+// shared memory and the other CTAs reach it through distributed shared memory
+// (atom / ld.shared::cluster through map_shared_rank; no TMA) -- so the
+// heaviest rows of a wide B stay on chip instead of falling to the global
+// bitmap bin.  Persistent: every cluster takes rows cid, cid + nclusters, ...
+// Per row:
+//   1. the CTAs split the row's A entries in slices of THREADS (CTA c takes
+//      slices c, c + csize, ...) and set each product's bit in the CTA that
+//      owns its column (local or remote atomicOr), and that CTA's summary bit;
+//   2. each CTA counts its slice's columns; the CTAs' counts, read across the
+//      cluster, give every CTA its first output position, and each CTA writes
+//      its sorted columns and block ranks (the bitmap bin's extraction);
+//   3. the CTAs walk their slices again: a product's position is the owning
+//      CTA's block rank plus the set bits before its own, read from the
+//      owner's shared memory, and its value goes to C.val by a global
+//      reduction;
+//   4. each CTA clears its own non-empty words.
+// Cluster barriers separate the steps (a remote bit set in step 1 is seen by
+// the owner's count; nothing clears a bitmap another CTA may still read).
+constexpr int kClusterBitmapMaxCtas = static_cast<int>(kClusterBitmapCols / kBitmapCols);
+
+template<typename V, int THREADS>
+__global__ __launch_bounds__(THREADS) void k_s2n_bitmap_cluster(ProductArgs p) {
+    using L = BitmapLayout<V, THREADS, kBitmapCols>;
+    constexpr int NW = THREADS / kWarp;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t* bm = reinterpret_cast<uint32_t*>(smem_raw);
+    uint32_t* summary = reinterpret_cast<uint32_t*>(smem_raw + L::bm_bytes);
+    int32_t* block_rank = reinterpret_cast<int32_t*>(smem_raw + L::bm_bytes + L::summary_bytes);
+    auto& sc = *reinterpret_cast<CtaScratch<THREADS>*>(smem_raw + L::bm_bytes +
+                                                        L::summary_bytes + L::rank_bytes);
+    __shared__ int32_t s_total;  // this CTA's column count of the current row
+    cg::cluster_group cluster = cg::this_cluster();
+    const int csize = static_cast<int>(cluster.num_blocks());
+    const int crank = static_cast<int>(cluster.block_rank());
+    const int nclusters = static_cast<int>(gridDim.x) / csize;
+    const int cid = static_cast<int>(blockIdx.x) / csize;
+    const int tid = threadIdx.x;
+    const int slice_lo = crank * kBitmapCols;  // first column this CTA holds
+    const int words = (min(kBitmapCols, max(0, p.n_cols - slice_lo)) + 31) >> 5;
+    for (int i = tid; i < words; i += THREADS) bm[i] = 0u;
+    summary[tid] = 0u;
+    cluster.sync();
+    const int w0 = tid * 32;  // this thread's bitmap words [w0, w0 + 32)
+    for (int rid = cid; rid < p.nrows; rid += nclusters) {
+        const int row = p.rows[rid];
+        const int c0 = p.c_rpt[row];
+        // the row's exact nnz, or in one-pass mode its NIP (an upper bound)
+        const int bound = p.c_rpt[row + 1] - c0;
+        const int a0 = p.a_rpt[row];
+        const int a1 = p.a_rpt[row + 1];
+        // 1. bits, each in the CTA that owns its column
+        for (int base = a0 + crank * THREADS; base < a1; base += csize * THREADS) {
+            cta_for_products_mlp<THREADS, kBitmapWalkU>(
+                p.a_col, p.b_rpt, base, min(base + THREADS, a1), sc,
+                [&](int qb, int, int) { return __ldg(p.b_col + qb); },
+                [&](int32_t key, int, int, int) {
+                    if (static_cast<uint32_t>(key) >= static_cast<uint32_t>(p.n_cols)) {
+                        report(p.status, kStBadInput, row, key);  // outside every slice
+                        return;
+                    }
+                    const int owner = key / kBitmapCols;
+                    const int wi = (key % kBitmapCols) >> 5;
+                    uint32_t* obm = owner == crank ? bm : cluster.map_shared_rank(bm, owner);
+                    if (atomicOr(obm + wi, 1u << (key & 31)) == 0u) {
+                        uint32_t* osum =
+                            owner == crank ? summary : cluster.map_shared_rank(summary, owner);
+                        atomicOr(osum + (wi >> 5), 1u << (wi & 31));
+                    }
+                });
+        }
+        cluster.sync();
+        // 2. count, place and extract this CTA's columns
+        const uint32_t sw = summary[tid];
+        int cnt = 0;
+        for (uint32_t m = sw; m != 0u; m &= m - 1u) cnt += __popc(bm[w0 + __ffs(m) - 1]);
+        const int inc = block_inclusive_scan<THREADS>(cnt, sc.warp_tot);
+        if (tid == 0) s_total = sc.warp_tot[NW - 1];
+        cluster.sync();
+        int before = 0;
+        int total = 0;
+        for (int r = 0; r < csize; r++) {
+            const int t = *cluster.map_shared_rank(&s_total, r);
+            total += t;
+            before += r < crank ? t : 0;
+        }
+        int pos = before + inc - cnt;
+        int32_t* cols = p.c_col + c0;
+#pragma unroll
+        for (int bb = 0; bb < 4; bb++) {
+            block_rank[(w0 >> 3) + bb] = pos;
+            for (uint32_t m = (sw >> (8 * bb)) & 0xffu; m != 0u; m &= m - 1u) {
+                const int wi = w0 + 8 * bb + __ffs(m) - 1;
+                for (uint32_t word = bm[wi]; word != 0u; word &= word - 1u) {
+                    if (pos < bound) cols[pos] = slice_lo + wi * 32 + __ffs(word) - 1;
+                    pos++;
+                }
+            }
+        }
+        int nnz = bound;
+        if (p.row_nnz != nullptr) {  // one-pass: the count is the row's nnz
+            nnz = total <= bound ? total : bound;
+            if (crank == 0 && tid == 0) p.row_nnz[row] = nnz;
+        } else if (total != nnz && crank == 0 && tid == 0) {
+            report(p.status, kStCapacity, row, total);
+        }
+        V* out = static_cast<V*>(p.c_val) + c0;
+        for (int i = crank * THREADS + tid; i < nnz; i += csize * THREADS) out[i] = V(0);
+        cluster.sync();  // every CTA's block ranks and the zeroed values are in place
+        // 3. values: positions from the owner's bitmap and block ranks
+        for (int base = a0 + crank * THREADS; base < a1; base += csize * THREADS) {
+            cta_for_products_mlp<THREADS, kBitmapWalkU>(
+                p.a_col, p.b_rpt, base, min(base + THREADS, a1), sc,
+                [&](int qb, int ai, int) {
+                    return KeyProduct<V>{__ldg(p.b_col + qb),
+                                         ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb)};
+                },
+                [&](const KeyProduct<V>& kp, int, int, int) {
+                    const int32_t key = kp.key;
+                    if (static_cast<uint32_t>(key) >= static_cast<uint32_t>(p.n_cols)) return;
+                    const int owner = key / kBitmapCols;
+                    const int wi = (key % kBitmapCols) >> 5;
+                    const int w8 = wi & ~7;
+                    const uint32_t* obm =
+                        owner == crank ? bm : cluster.map_shared_rank(bm, owner);
+                    const int32_t* orank =
+                        owner == crank ? block_rank : cluster.map_shared_rank(block_rank, owner);
+                    int rank = orank[wi >> 3] + __popc(obm[wi] & ((1u << (key & 31)) - 1u));
+#pragma unroll
+                    for (int t = 0; t < 7; t++)
+                        if (w8 + t < wi) rank += __popc(obm[w8 + t]);
+                    if (rank < nnz) atomicAdd(out + rank, kp.prod);
+                });
+        }
+        cluster.sync();  // no CTA reads another's bitmap any more
+        // 4. clear this CTA's words for the next row
+        for (uint32_t m = sw; m != 0u; m &= m - 1u) bm[w0 + __ffs(m) - 1] = 0u;
+        summary[tid] = 0u;
+        cluster.sync();  // cleared before any CTA sets the next row's bits
     }
 }
 
@@ -653,12 +844,67 @@ cudaError_t launch_cta(const ProductArgs& p, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// Order a bin's row list by slot size (the row's NIP in one-pass mode, its
+// nnz in two), largest first, ties by row: one CTA, a bitonic sort of
+// (INT32_MAX - size) << 32 | row keys in shared memory.  With the persistent
+// bins taking rows from a counter, the CTAs then finish together (largest
+// first: each CTA's last row is a short one).
+constexpr int kSortRowsMax = 8192;
+constexpr int kSortThreads = 1024;
+
+__global__ __launch_bounds__(kSortThreads) void k_rows_largest_first(int32_t* __restrict__ rows,
+                                                                     int32_t n,
+                                                                     const int32_t* __restrict__ c_rpt) {
+    extern __shared__ unsigned long long s_key[];
+    int N = 1;
+    while (N < n) N <<= 1;
+    for (int i = threadIdx.x; i < N; i += kSortThreads) {
+        unsigned long long k = ~0ull;
+        if (i < n) {
+            const int r = rows[i];
+            const int size = c_rpt[r + 1] - c_rpt[r];
+            k = (static_cast<unsigned long long>(static_cast<uint32_t>(INT32_MAX - size)) << 32) |
+                static_cast<uint32_t>(r);
+        }
+        s_key[i] = k;
+    }
+    __syncthreads();
+    for (int k = 2; k <= N; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < (N >> 1); i += kSortThreads) {
+                const int lo = 2 * i - (i & (j - 1));
+                const int hi = lo + j;
+                const bool up = (lo & k) == 0;
+                const unsigned long long a = s_key[lo];
+                const unsigned long long b = s_key[hi];
+                if ((a > b) == up) {
+                    s_key[lo] = b;
+                    s_key[hi] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = threadIdx.x; i < n; i += kSortThreads)
+        rows[i] = static_cast<int32_t>(s_key[i] & 0xffffffffull);
+}
+
 template<typename V, int THREADS, int CAP>
 cudaError_t launch_bitmap(const ProductArgs& p, cudaStream_t s) {
     // persistent: one CTA per SM at most (the bitmap takes most of an SM's
     // shared memory)
     const int sms = p.sm_count > 0 ? p.sm_count : 148;
     const int grid = p.nrows < sms ? p.nrows : sms;
+    if (p.work != nullptr) {
+        // the bin's row list is the library's own (a binning pass wrote it)
+        if (p.nrows > grid && p.nrows <= kSortRowsMax) {
+            k_rows_largest_first<<<1, kSortThreads, sizeof(unsigned long long) * kSortRowsMax, s>>>(
+                const_cast<int32_t*>(p.rows), p.nrows, p.c_rpt);
+            if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return e;
+        }
+        if (cudaError_t e = cudaMemsetAsync(p.work, 0, sizeof(int32_t), s); e != cudaSuccess)
+            return e;
+    }
     k_s2n_bitmap<V, THREADS, CAP><<<grid, THREADS, BitmapLayout<V, THREADS, CAP>::bytes, s>>>(p);
     return cudaGetLastError();
 }
@@ -668,6 +914,40 @@ cudaError_t launch_global(const ProductArgs& p, cudaStream_t s) {
     const int grid = p.nrows < p.nmaps ? p.nrows : p.nmaps;
     k_s2n_global<V, THREADS><<<grid, THREADS, 0, s>>>(p);
     return cudaGetLastError();
+}
+
+// Cluster bitmap bin: a cluster of ceil(B.n / 2^20) CTAs (at most 8) per row
+// in flight, as many clusters as fit on the device at once.  B.n beyond the
+// cluster's reach, or no cluster of that size resident, runs the rows in the
+// global bitmap bin instead.
+template<typename V, int THREADS>
+cudaError_t launch_bitmap_cluster(const ProductArgs& p, cudaStream_t s) {
+    const int64_t need = (static_cast<int64_t>(p.n_cols) + kBitmapCols - 1) / kBitmapCols;
+    if (need < 1 || need > kClusterBitmapMaxCtas) return launch_global<V, THREADS>(p, s);
+    const int csize = static_cast<int>(need);
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(THREADS);
+    cfg.dynamicSmemBytes = BitmapLayout<V, THREADS, kBitmapCols>::bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = static_cast<unsigned>(csize);
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const int sms = p.sm_count > 0 ? p.sm_count : 148;
+    cfg.gridDim = dim3(static_cast<unsigned>(csize * (sms / csize)));
+    int resident = 0;
+    if (cudaOccupancyMaxActiveClusters(&resident, k_s2n_bitmap_cluster<V, THREADS>, &cfg) !=
+            cudaSuccess ||
+        resident <= 0) {
+        (void)cudaGetLastError();  // clear a failed query; the global bin takes the rows
+        return launch_global<V, THREADS>(p, s);
+    }
+    const int nclusters = p.nrows < resident ? p.nrows : resident;
+    cfg.gridDim = dim3(static_cast<unsigned>(csize * nclusters));
+    return cudaLaunchKernelEx(&cfg, k_s2n_bitmap_cluster<V, THREADS>, p);
 }
 
 template<typename V>
@@ -693,6 +973,8 @@ struct S2nLadder {
          "s2n_cta512_t16384", launch_cta<V, 512, 16384, 12288>},                              \
         {BinKind::Cta, 32768, 1, 1024, CtaLayout<1024, 43008, 32768>::bytes,                  \
          "s2n_cta1024_t43008", launch_cta<V, 1024, 43008, 32768>},                            \
+        {BinKind::Cluster, INT32_MAX, 1, 1024, BitmapLayout<V, 1024, kBitmapCols>::bytes,     \
+         "s2n_bitmap_cluster", launch_bitmap_cluster<V, 1024>},                               \
         {BinKind::Global, INT32_MAX, 1, 1024, 0, "s2n_global_bitmap", launch_global<V, 1024>}, \
     };                                                                                        \
     template<>                                                                                \
@@ -774,6 +1056,7 @@ cudaError_t prepare_one() {
     B200_SMEM((k_s2n_cta<V, 512, 16384, 12288>), (CtaLayout<512, 16384, 12288>::bytes));
     B200_SMEM((k_s2n_cta<V, 1024, 43008, 32768>), (CtaLayout<1024, 43008, 32768>::bytes));
     B200_SMEM((k_s2n_bitmap<V, 1024, kBitmapCols>), (BitmapLayout<V, 1024, kBitmapCols>::bytes));
+    B200_SMEM((k_s2n_bitmap_cluster<V, 1024>), (BitmapLayout<V, 1024, kBitmapCols>::bytes));
     B200_SMEM((k_esc_team<V, 4, 256, 12>), (EscLayout<V, 4, 256, 12>::bytes));
     B200_SMEM((k_esc_team<V, 8, 256, 48>), (EscLayout<V, 8, 256, 48>::bytes));
     B200_SMEM((k_esc_team<V, 16, 256, 192>), (EscLayout<V, 16, 256, 192>::bytes));
@@ -844,7 +1127,10 @@ cudaError_t launch_esc_decide(EscSample* sample, const Ladder& base, int esc_mod
 }
 
 cudaError_t s2n_prepare() {
-    cudaError_t e = prepare_one<double>();
+    cudaError_t e = cudaFuncSetAttribute(k_rows_largest_first,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(sizeof(unsigned long long) * kSortRowsMax));
+    if (e == cudaSuccess) e = prepare_one<double>();
     if (e == cudaSuccess) e = prepare_one<float>();
     return e;
 }

@@ -63,6 +63,9 @@ struct ProductArgs {
     int32_t* row_nnz;
     // SMs of the device (persistent kernels size their grid by it; 0: 148)
     int32_t sm_count;
+    // persistent bins: a device counter the CTAs take their next row from
+    // (the launcher zeroes it; nullptr: rows dealt out by CTA index)
+    int32_t* work;
 };
 
 enum class BinKind : int { Team = 0, Cta = 1, Cluster = 2, Global = 3 };
@@ -90,6 +93,9 @@ int s2n_ladder_f64(const BinLauncher** out);
 int s2n_ladder_f32(const BinLauncher** out);
 // The same for B.n <= kBitmapCols, whose large rows use a shared-memory bitmap.
 constexpr int kBitmapCols = 1 << 20;
+// The wide ladder's cluster bitmap bin holds up to this many columns (8 CTAs
+// of kBitmapCols); past it its rows run in the global bitmap bin.
+constexpr int64_t kClusterBitmapCols = int64_t(8) * kBitmapCols;
 int s2n_bitmap_ladder_f64(const BinLauncher** out);
 int s2n_bitmap_ladder_f32(const BinLauncher** out);
 // One-pass ladder for B.n <= kBitmapCols (key = NIP of the row): the team bins

@@ -64,6 +64,7 @@ struct Scratch {
     int32_t* fail_count;
     EscSample* sample;
     Ladder* dladder;  // the one-pass fill binning's limits, decided on the device
+    int32_t* work;    // one row counter per fill bin (persistent bins)
 };
 
 struct ProfRec {
@@ -191,6 +192,7 @@ spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s, cudaStre
     const size_t o_bins1 = take(sizeof(int32_t) * mm);
     const size_t o_bins2 = take(sizeof(int32_t) * mm);
     const size_t o_fail = take(sizeof(int32_t) * mm);
+    const size_t o_work = take(sizeof(int32_t) * kMaxBins);
     if (spgemm_status st = regrow(h, &h->scratch, &h->scratch_bytes, off + off / 4, stream);
         st != SPGEMM_OK)
         return st;
@@ -207,6 +209,7 @@ spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s, cudaStre
     s->bins1 = reinterpret_cast<int32_t*>(b + o_bins1);
     s->bins2 = reinterpret_cast<int32_t*>(b + o_bins2);
     s->fail_rows = reinterpret_cast<int32_t*>(b + o_fail);
+    s->work = reinterpret_cast<int32_t*>(b + o_work);
     return SPGEMM_OK;
 }
 
@@ -223,6 +226,17 @@ spgemm_status ensure_bitmaps(spgemm_handle_s* h, int64_t words, int32_t rows, in
         return st;
     *nmaps = static_cast<int32_t>(n);
     return SPGEMM_OK;
+}
+
+// Rows of a fill plan that may need the global bins' bitmaps: the global
+// bin's, and the cluster bitmap bin's when B.n is past the columns a cluster
+// holds (that bin then hands its rows to the global kernel).
+int32_t global_bitmap_rows(const BinLauncher* bins, int nb, const Plan& plan, int32_t n) {
+    int32_t rows = plan.bin_size[nb - 1];
+    if (nb >= 2 && bins[nb - 2].kind == BinKind::Cluster &&
+        static_cast<int64_t>(n) > kClusterBitmapCols)
+        rows = std::max(rows, plan.bin_size[nb - 2]);
+    return rows;
 }
 
 Ladder make_ladder(const BinLauncher* bins, int nb, int min_bin) {
@@ -355,6 +369,7 @@ spgemm_status launch_bins(spgemm_handle_s* h, const BinLauncher* bins, int nb, i
         ProductArgs a = base;
         a.rows = row_lists + plan.bin_off[b];
         a.nrows = rows;
+        a.work = base.work != nullptr ? base.work + b : nullptr;
         cudaStream_t s = h->side[next % h->nside];
         next++;
         const BinLauncher& L = bins[b];
@@ -374,18 +389,26 @@ spgemm_status launch_bins(spgemm_handle_s* h, const BinLauncher* bins, int nb, i
 // products); otherwise hand it back in `graph` (batch groups).
 struct CaptureReq {
     double team_scale = 1.0;
+    double cta_scale = 1.0;  // the same for the CTA bins (block size and table of a row)
     spgemm_plan_s* plan = nullptr;
     bool launch_now = true;
     cudaGraph_t graph = nullptr;
 };
 
-Ladder scaled_ladder(const BinLauncher* bins, int nb, int min_bin, double team_scale) {
+Ladder scaled_ladder(const BinLauncher* bins, int nb, int min_bin, double team_scale,
+                     double cta_scale = 1.0) {
     Ladder l = make_ladder(bins, nb, min_bin);
-    if (team_scale >= 1.0) return l;
+    if (team_scale >= 1.0 && cta_scale >= 1.0) return l;
     int prev = 0;
     for (int i = 0; i < nb; i++) {
-        if (bins[i].kind == BinKind::Team) {
-            const int lim = static_cast<int>(bins[i].limit * team_scale);
+        // the team bins' limits by team_scale, the CTA bins' by cta_scale
+        // (the bitmap bin, whose limit is the column count, keeps it)
+        const double sc = bins[i].kind == BinKind::Team ? team_scale
+                          : (bins[i].kind == BinKind::Cta && bins[i].limit < kBitmapCols)
+                              ? cta_scale
+                              : 1.0;
+        if (sc < 1.0) {
+            const int lim = static_cast<int>(bins[i].limit * sc);
             l.limit[i] = lim > prev ? lim : prev + 1;  // limits stay increasing
         }
         prev = l.limit[i];
@@ -492,16 +515,11 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     // ---- count pass: NIP per row and bins ---------------------------------
     const int nctas = bin_ctas(m);
     const Ladder lad1 = make_ladder(sym, nsym, h->min_sym_bin);
-    B200_STEP(timed(h, "nip_hist", 0, -1, m, stream, [&](cudaStream_t ss) {
-        return launch_nip_hist(A->rpt, A->col, B->rpt, m, c_rpt, s.hist1, s.plan1, s.status,
-                               lad1, ss);
-    }));
     // Compression sample (products that may run one pass): it reads A and B
-    // only and runs on a side stream after the NIP pass, beside the NIP
-    // binning and the host's first synchronisation, then decides the one-pass
-    // fill binning's limits on the device.  Its sums come back with the fill
-    // binning's plan: they choose one pass or two and, per fill bin,
-    // expand-sort-compress or hashing.
+    // only, so it runs on a side stream beside the NIP pass (forked before
+    // it), then decides the one-pass fill binning's limits on the device.
+    // Its sums come back with the fill binning's plan: they choose one pass
+    // or two and, per fill bin, expand-sort-compress or hashing.
     const Ladder ladf = make_ladder(fil, nfil, h->min_num_bin);
     const int esc_mode = (narrow && h->esc != 2) ? h->esc : 2;
     const bool sampled = cr == nullptr && h->one_pass != 2 && A->nnz >= kSampleMinNnz &&
@@ -533,6 +551,10 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         if (cudaError_t e = cudaEventRecord(h->ev_sample, side); e != cudaSuccess)
             return bail(cuda_fail(e, "join the sample stream"));
     }
+    B200_STEP(timed(h, "nip_hist", 0, -1, m, stream, [&](cudaStream_t ss) {
+        return launch_nip_hist(A->rpt, A->col, B->rpt, m, c_rpt, s.hist1, s.plan1, s.status,
+                               lad1, ss);
+    }));
     // The fill binning by NIP (the one-pass path's), with limits decided on
     // the device when the sample ran: off = the scan of the NIP per row.
     int32_t* off = nullptr;
@@ -605,6 +627,7 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     pa.fail_count = s.fail_count;
     pa.words = (static_cast<int64_t>(n) + 31) / 32;
     pa.sm_count = h->sm_count;
+    pa.work = s.work;
 
     // ---- one-pass fill: no count phase ------------------------------------
     // Rows are binned by NIP (an upper bound of their nnz) on the fill ladder
@@ -713,9 +736,9 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         pa.c_col = tmp_col;
         pa.c_val = tmp_val;
         pa.row_nnz = c_rpt;
-        if (pf.bin_size[nfil - 1] > 0) {
+        if (const int32_t gr = global_bitmap_rows(fil, nfil, pf, n); gr > 0) {
             int32_t nmaps = 0;
-            B200_ONE(ensure_bitmaps(h, pa.words, pf.bin_size[nfil - 1], &nmaps, stream));
+            B200_ONE(ensure_bitmaps(h, pa.words, gr, &nmaps, stream));
             pa.bitmaps = h->bitmaps;
             pa.nmaps = nmaps;
         }
@@ -846,7 +869,8 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     B200_STEP(join_streams(h, stream));
 
     // ---- scan pass: row pointer and fill bins -------------------------------
-    const Ladder lad2 = scaled_ladder(fil, nfil, h->min_num_bin, cr ? cr->team_scale : 1.0);
+    const Ladder lad2 = scaled_ladder(fil, nfil, h->min_num_bin, cr ? cr->team_scale : 1.0,
+                                      cr ? cr->cta_scale : 1.0);
     B200_STEP(timed(h, "nnz_hist", 2, -1, m, stream, [&](cudaStream_t ss) {
         return launch_nnz_hist(c_rpt, m, s.hist2, s.cta_sum, s.plan2, lad2, ss);
     }));
@@ -889,9 +913,9 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         return bail(cuda_fail(e, "allocate C.val"));
     pa.c_col = C->col;
     pa.c_val = C->val;
-    if (p2.bin_size[nfil - 1] > 0) {
+    if (const int32_t gr = global_bitmap_rows(fil, nfil, p2, n); gr > 0) {
         int32_t nmaps = 0;
-        B200_STEP(ensure_bitmaps(h, pa.words, p2.bin_size[nfil - 1], &nmaps, stream));
+        B200_STEP(ensure_bitmaps(h, pa.words, gr, &nmaps, stream));
         pa.bitmaps = h->bitmaps;
         pa.nmaps = nmaps;
     }
@@ -914,6 +938,10 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
                                  stream));
             pa.bitmaps = static_cast<uint32_t*>(bm);
         }
+        int32_t* work = nullptr;  // the persistent bins' row counters
+        B200_STEP(plan_alloc(plan, reinterpret_cast<void**>(&work), sizeof(int32_t) * kMaxBins,
+                             stream));
+        pa.work = work;
         pa.status = plan->status;
         fill_status = plan->status;
         const int saved_profile = h->profile;
@@ -967,7 +995,8 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
 template<typename V>
 spgemm_status batch(spgemm_handle_s* h, const spgemm_batch_desc* d, const spgemm_csr_view* A,
                     const spgemm_csr_view* B, spgemm_batch_out* out, cudaStream_t stream,
-                    spgemm_plan_s* plan = nullptr, double team_scale = 1.0) {
+                    spgemm_plan_s* plan = nullptr, double team_scale = 1.0,
+                    double cta_scale = 1.0) {
     if (h == nullptr || d == nullptr || out == nullptr)
         return fail(SPGEMM_ERR_INVALID_ARG, "NULL argument");
     std::memset(out, 0, sizeof(*out));
@@ -1086,6 +1115,7 @@ spgemm_status batch(spgemm_handle_s* h, const spgemm_batch_desc* d, const spgemm
         spgemm_csr_out Cg;
         CaptureReq cr;
         cr.team_scale = team_scale;
+        cr.cta_scale = cta_scale;
         cr.plan = plan;
         cr.launch_now = false;
         spgemm_status st = product<V>(h, &Ag, B, &Cg, stream, &cr);
@@ -1564,27 +1594,37 @@ spgemm_status plan_time(spgemm_plan_s* p, cudaStream_t stream, float* ms) {
     return SPGEMM_OK;
 }
 
-// Build a plan with `make(plan, team_scale)` -- a product or a batch in plan
-// mode, which also fills the caller's output -- once with the default
-// configuration, or, when tuning, once per candidate (team bins' routing
-// scale x side streams), keeping the fastest replay.  `drop` frees the output
-// of a candidate that loses.
+// Build a plan with `make(plan, team_scale, cta_scale)` -- a product or a
+// batch in plan mode, which also fills the caller's output -- once with the
+// default configuration, or, when tuning, once per candidate, keeping the
+// fastest replay.  The candidates: the team bins' routing limits scaled by
+// 1, 0.75 or 0.5 (a row then runs with a larger hash table and more lanes),
+// the CTA bins' by 1 or 0.5 (a larger table and block: 256 -> 512 -> 1,024
+// threads), and 4 or 8 side streams (parallel branches of the graph).  `drop`
+// frees the output of a candidate that loses.
 template<typename Make, typename Drop>
 spgemm_status plan_build(spgemm_handle_s* h, int tune, cudaStream_t stream, Make&& make,
                          Drop&& drop, spgemm_plan_s** out) {
     static constexpr double kScales[] = {1.0, 0.75, 0.5};
+    static constexpr double kCtaScales[] = {1.0, 0.5};
     static constexpr int kStreams[] = {4, 8};
     struct Cand {
         double scale;
+        double cta;
         int streams;
     };
     std::vector<Cand> cands;
     if (tune) {
         for (double sc : kScales)
-            for (int ns : kStreams) cands.push_back({sc, ns});
+            for (double cs : kCtaScales)
+                for (int ns : kStreams) cands.push_back({sc, cs, ns});
     } else {
-        cands.push_back({1.0, h->nside});
+        cands.push_back({1.0, 1.0, h->nside});
     }
+    static_assert(sizeof(kScales) / sizeof(double) * sizeof(kCtaScales) / sizeof(double) *
+                          sizeof(kStreams) / sizeof(int) <=
+                      SPGEMM_PLAN_MAX_CANDIDATES,
+                  "plan info holds every candidate");
     const int saved_nside = h->nside;
     spgemm_plan_s* best = nullptr;
     int best_i = -1;
@@ -1595,7 +1635,7 @@ spgemm_status plan_build(spgemm_handle_s* h, int tune, cudaStream_t stream, Make
         h->nside = cands[i].streams;
         spgemm_plan_s* p = nullptr;
         st = plan_new(h, &p, stream);
-        if (st == SPGEMM_OK) st = make(p, cands[i].scale);
+        if (st == SPGEMM_OK) st = make(p, cands[i].scale, cands[i].cta);
         float ms = 0.0f;
         if (st == SPGEMM_OK) st = plan_time(p, stream, &ms);
         if (st != SPGEMM_OK) {
@@ -1604,6 +1644,7 @@ spgemm_status plan_build(spgemm_handle_s* h, int tune, cudaStream_t stream, Make
             break;
         }
         info.team_scale[i] = static_cast<float>(cands[i].scale);
+        info.cta_scale[i] = static_cast<float>(cands[i].cta);
         info.streams[i] = cands[i].streams;
         info.ms[i] = ms;
         if (best == nullptr || ms < info.ms[best_i]) {
@@ -1679,9 +1720,10 @@ spgemm_status plan_csr(spgemm_handle_t h, const spgemm_csr_view* A, const spgemm
     B200_TRY(cudaSetDevice(h->device));
     // the kept plan's output is in *C; a losing candidate's output is freed
     spgemm_csr_out cur = {};
-    auto make = [&](spgemm_plan_s* p, double scale) {
+    auto make = [&](spgemm_plan_s* p, double scale, double cta) {
         CaptureReq cr;
         cr.team_scale = scale;
+        cr.cta_scale = cta;
         cr.plan = p;
         cr.launch_now = true;
         return product<V>(h, A, B, &cur, s, &cr);
@@ -1697,8 +1739,8 @@ spgemm_status plan_csr(spgemm_handle_t h, const spgemm_csr_view* A, const spgemm
     spgemm_plan_s* p = nullptr;
     // plan_build calls make() then drop(); the first candidate becomes the best
     // without a drop, so move its output into *C right after
-    auto make_first = [&](spgemm_plan_s* pl, double scale) {
-        const spgemm_status st = make(pl, scale);
+    auto make_first = [&](spgemm_plan_s* pl, double scale, double cta) {
+        const spgemm_status st = make(pl, scale, cta);
         if (st == SPGEMM_OK && C->rpt == nullptr) *C = cur;
         return st;
     };
@@ -1719,8 +1761,8 @@ spgemm_status plan_batch(spgemm_handle_t h, const spgemm_batch_desc* d, const sp
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     B200_TRY(cudaSetDevice(h->device));
     spgemm_batch_out cur = {};
-    auto make = [&](spgemm_plan_s* p, double scale) {
-        const spgemm_status st = batch<V>(h, d, A, B, &cur, s, p, scale);
+    auto make = [&](spgemm_plan_s* p, double scale, double cta) {
+        const spgemm_status st = batch<V>(h, d, A, B, &cur, s, p, scale, cta);
         if (st == SPGEMM_OK && out->products == nullptr) *out = cur;
         return st;
     };

@@ -9,20 +9,23 @@ stream), repeatedly
    binning phase's upper bound on the output,
    ``bytes(C) <= 4 (m + 1) + NIP * (4 + sizeof(value))``, is the request's
    share of the memory budget;
-2. admit, oldest first: a request with ``NIP >= solo_nip`` fills the GPU by
-   itself and runs alone on the plain path; smaller ones are taken in arrival
-   order (passing over large ones, which the next admission takes) while the
-   budget, ``max_batch`` and the per-batch NIP cap ``batch_nip`` allow;
+2. admit, oldest first: a request with ``NIP >= solo_nip`` runs alone on the
+   plain path (its rows already fill every bin); smaller ones are taken in
+   arrival order (passing over large ones, which the next free worker takes)
+   while the budget, ``max_batch`` and the per-batch NIP cap ``batch_nip`` --
+   which bounds a batch's duration, so a small request never waits long for
+   the rest of its batch -- allow;
 3. pack the small requests into block-diagonal operands and run them as ONE
    batched product (``spgemm_batch_*``), so rows of different requests share
    bins and kernels;
 4. hand each request its own CSR result and release its share of the budget.
 
-Large products gain nothing from packing (their rows already fill every bin),
-and a small request packed with one would wait for it, so the two kinds are
-never mixed.  With two workers a large product and a batch of small ones run
-side by side on the GPU.  The reference has no served or batched form; it
-multiplies one pair per call (proposal.cuh:85-124).
+Workers wait on one condition variable that every arrival, every finished
+sizing and every finished unit signals, and a free worker always takes the
+next unit at once: with several workers a large product, medium products and
+batches of small ones run side by side on the GPU, each on its worker's
+stream.  The reference has no served or batched form; it multiplies one pair
+per call (proposal.cuh:85-124).
 """
 from __future__ import annotations
 
@@ -61,17 +64,27 @@ class SpgemmServer:
 
     memory_budget: bytes of C bounds that may be in flight at once.
     max_batch:     most requests packed into one batched product.
-    workers:       worker threads (handles); 2 lets batches overlap.
+    workers:       worker threads (handles), each with its own stream: units
+                   of work run side by side on the GPU.
     solo_nip:      requests with at least this many intermediate products run
                    alone on the plain path.
-    batch_nip:     cap on the intermediate products of one batch (bounds the
-                   time a batch's first request waits for its last).
+    batch_nip:     most intermediate products of one batch.  The cap a batch
+                   actually gets follows the backlog: the queued requests' NIP
+                   shared over the workers, at least batch_nip_min.  A short
+                   queue (light load) makes short batches, so a small request
+                   does not wait long for the rest of its batch; a long one
+                   (saturation) makes long batches, which amortise each
+                   product's fixed cost over many requests.
+    batch_cols:    most columns of a packed batch's B (the sum of its
+                   members' B.n): up to 2^20 the batch runs the bitmap and
+                   expand-sort-compress fill bins.
     size_chunk:    most arrivals a worker sizes in one call before it tries to
                    admit.
     """
 
     def __init__(self, memory_budget: int = 32 << 30, max_batch: int = 256, workers: int = 2,
                  device: int = 0, solo_nip: int = 4 << 20, batch_nip: int = 32 << 20,
+                 batch_nip_min: int = 4 << 20, batch_cols: int = 1 << 20,
                  size_chunk: int = 256):
         import torch
         self._torch = torch
@@ -80,6 +93,9 @@ class SpgemmServer:
         self.max_batch = int(max_batch)
         self.solo_nip = int(solo_nip)
         self.batch_nip = int(batch_nip)
+        self.batch_nip_min = int(batch_nip_min)
+        self.batch_cols = int(batch_cols)
+        self.workers = int(workers)
         self.size_chunk = int(size_chunk)
         self._queue: deque[Request] = deque()
         self._cv = threading.Condition()
@@ -124,12 +140,16 @@ class SpgemmServer:
     def _admit(self) -> tuple[list[Request], bool]:
         """Take the next unit of work (call with the lock held): a large
         request alone (second value True), or small requests in arrival order
-        under the budget, max_batch and batch_nip.  Unsized requests stop the
+        under the budget, max_batch, the backlog-scaled NIP cap and
+        batch_cols.  Unsized requests stop the
         scan, so admission order is arrival order.  A request larger than the
         whole budget runs when nothing else is in flight."""
         taken: list[Request] = []
         nip = 0
+        cols = 0
         skipped = []
+        backlog = sum(r.nip for r in self._queue if r.bound_bytes >= 0 and r.nip < self.solo_nip)
+        cap = max(self.batch_nip_min, min(self.batch_nip, backlog // max(1, self.workers)))
         while self._queue and len(taken) < self.max_batch:
             r = self._queue[0]
             if r.bound_bytes < 0:
@@ -147,16 +167,38 @@ class SpgemmServer:
                 return [r], True
             if not fits and (taken or self._in_flight_bytes > 0):
                 break
-            if taken and nip + r.nip > self.batch_nip:
+            if taken and (nip + r.nip > cap or cols + r.B.n > self.batch_cols):
                 break
             self._queue.popleft()
             self._in_flight_bytes += r.bound_bytes
             nip += r.nip
+            cols += r.B.n
             taken.append(r)
             if not fits:
                 break
         self._queue.extendleft(reversed(skipped))
         return taken, False
+
+    def _next(self) -> tuple[list[Request], list[Request], bool]:
+        """Block until this worker has something to do (call with the lock
+        held): requests to size, or a unit of work.  Returns (unsized, unit,
+        solo); both lists empty means stop."""
+        while True:
+            if self._stop and not self._queue:
+                return [], [], False
+            unsized = []
+            for r in self._queue:
+                if r.bound_bytes < 0 and not r.sizing:
+                    r.sizing = True
+                    unsized.append(r)
+                    if len(unsized) == self.size_chunk:
+                        break
+            if unsized:
+                return unsized, [], False
+            unit, solo = self._admit()
+            if unit:
+                return [], unit, solo
+            self._cv.wait()
 
     def _worker(self, wid: int, handle: Handle) -> None:
         torch = self._torch
@@ -164,20 +206,12 @@ class SpgemmServer:
         stream = torch.cuda.Stream(device=self.device)
         while True:
             with self._cv:
-                while not self._stop and not self._queue:
-                    self._cv.wait()
-                if self._stop and not self._queue:
-                    return
-                unsized = []
-                for r in self._queue:
-                    if r.bound_bytes < 0 and not r.sizing:
-                        r.sizing = True
-                        unsized.append(r)
-                        if len(unsized) == self.size_chunk:
-                            break
+                unsized, reqs, solo = self._next()
+            if not unsized and not reqs:
+                return
             if unsized:
                 # admission bounds of new arrivals: one sizing launch, on this
-                # worker's stream
+                # worker's stream; then this worker admits
                 try:
                     nips = get_nip_many([(r.A, r.B) for r in unsized], handle, stream)
                 except BaseException as e:  # an invalid pair fails the whole call
@@ -189,12 +223,7 @@ class SpgemmServer:
                     r.bound_bytes = 4 * (r.A.m + 1) + nip * (4 + r.A.val.element_size())
                 with self._cv:
                     self._cv.notify_all()
-            with self._cv:
-                reqs, solo = self._admit()
-                if not reqs:
-                    if not unsized:
-                        self._cv.wait(timeout=0.0005)
-                    continue
+                continue
             now = time.perf_counter()
             for r in reqs:
                 r.t_admitted = now

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define SPGEMM_ABI_VERSION 4
+#define SPGEMM_ABI_VERSION 5
 
 #if defined(__GNUC__)
 #define SPGEMM_API __attribute__((visibility("default")))
@@ -328,12 +328,17 @@ SPGEMM_API spgemm_status spgemm_batch_free(spgemm_batch_out* out, void* stream);
  * the reference, which recomputes the structure on every call. */
 typedef struct spgemm_plan_s* spgemm_plan_t;
 
+#define SPGEMM_PLAN_MAX_CANDIDATES 16
+
 typedef struct spgemm_plan_info {
     int32_t candidates;   /* configurations built (1 without tuning) */
     int32_t chosen;       /* index of the one the plan keeps */
-    float team_scale[8];  /* routing limits of the team fill bins x this */
-    int32_t streams[8];   /* side streams = parallel branches of the graph */
-    float ms[8];          /* median replay time of each configuration */
+    float team_scale[SPGEMM_PLAN_MAX_CANDIDATES]; /* routing limits of the team fill bins x this
+                                                     (the hash table and lanes a row gets) */
+    float cta_scale[SPGEMM_PLAN_MAX_CANDIDATES];  /* the same for the CTA fill bins (the table
+                                                     and block size a row gets) */
+    int32_t streams[SPGEMM_PLAN_MAX_CANDIDATES];  /* side streams = parallel graph branches */
+    float ms[SPGEMM_PLAN_MAX_CANDIDATES];         /* median replay time of each */
 } spgemm_plan_info;
 
 SPGEMM_API spgemm_status spgemm_plan_csr_f64(spgemm_handle_t handle, const spgemm_csr_view* A,

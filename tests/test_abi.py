@@ -25,7 +25,8 @@ def test_library_exports_every_symbol(native_lib):
 
 
 def test_status_strings_and_version(native_lib):
-    assert native_lib.spgemm_abi_version() == 4
+    from gpuspgemm_b200 import _native as N
+    assert native_lib.spgemm_abi_version() == N.ABI_VERSION == 5
     assert native_lib.spgemm_status_string(0) == b"SPGEMM_OK"
     assert native_lib.spgemm_status_string(4) == b"SPGEMM_ERR_OVERFLOW"
 

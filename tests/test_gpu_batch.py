@@ -71,6 +71,46 @@ def test_batch_packed_gpu_generator_and_groups(handle, oracle_mod):
     torch.cuda.synchronize()
 
 
+def _packed_member(M, off, i):
+    """Product i's square operand, in local indices, from a packed operand
+    (device tensors sliced on the device, then copied)."""
+    r0, r1 = int(off[i]), int(off[i + 1])
+    rpt = M.rpt[r0:r1 + 1].cpu().numpy()
+    s0, s1 = int(rpt[0]), int(rpt[-1])
+    return HostCSR(r1 - r0, r1 - r0, (rpt - s0).astype(np.int32),
+                   (M.col[s0:s1].cpu().numpy() - r0).astype(np.int32),
+                   M.val[s0:s1].cpu().numpy().astype(np.float64))
+
+
+def test_full_batched_workload_sampled_parity(handle, oracle_mod):
+    """The batched workload at its stated size: 4,096 independent FP32
+    products (rows log-uniform in [64, 16384], Poisson(U[6, 40]) nnz per row,
+    ~6.8 G nonzeros of C) run as one batch; 48 products drawn at random, plus
+    the largest and the smallest, checked against the oracle."""
+    import torch
+
+    from gpuspgemm_b200.api import PackedBatch, batch
+    a_off, b_off, c_off, A, B = G.batch_packed_gpu(4096, seed=20261203, dtype=torch.float32)
+    pb = PackedBatch(a_off, b_off, c_off, A, B)
+    out = batch(pb, handle)
+    assert len(out) == 4096
+    assert sum(c.nnz for c in out) > 6_000_000_000
+    sizes = np.diff(np.asarray(a_off))
+    rng = np.random.default_rng(77)
+    picks = set(rng.choice(4096, 48, replace=False).tolist())
+    picks |= {int(np.argmax(sizes)), int(np.argmin(sizes))}
+    for i in sorted(picks):
+        Ai = _packed_member(A, a_off, i)
+        Bi = _packed_member(B, b_off, i)
+        R = oracle_mod.spgemm(Ai, Bi, np.float64)
+        ch = out[i].to_host()
+        res = oracle_mod.compare(ch, R, oracle_mod.abs_bound(Ai, Bi, R))
+        assert res["rpt_equal"] and res["col_equal"], (i, res)
+        assert res["max_cond"] <= 1e-5, (i, res)
+    del out
+    torch.cuda.synchronize()
+
+
 def test_get_nip_many_matches_single_calls(handle, oracle_mod):
     """One-launch sizing of many pairs: empty A, a pair larger than one CTA's
     chunk (16384 A entries), rectangular pairs."""

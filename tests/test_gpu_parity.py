@@ -210,6 +210,59 @@ def test_long_rows_wide_cta_bins(handle, oracle_mod, dtype):
 
 
 @pytest.mark.parametrize("passes", [1, 2])
+@pytest.mark.parametrize("ncols", [(1 << 21) + 7, 5_000_011, (1 << 23) + 3])
+def test_heaviest_wide_rows_in_cluster_bitmaps(handle, oracle_mod, passes, ncols):
+    """Rows of ~40k-200k distinct columns, past the largest CTA bin (32,768),
+    over a B of 2^21 + 7, 5.0 M or 2^23 + 3 columns: the cluster bitmap bin
+    holds each row's bitmap in the shared memory of a cluster of 3, 5 or 8 CTAs
+    (columns split by 2^20 per CTA, reached through distributed shared
+    memory).  A B of 9 M columns is past 8 CTAs: those rows run in the global
+    bitmap bin (test_rows_past_the_cluster_bitmaps_run_global)."""
+    from gpuspgemm_b200 import _native as N
+    rng = np.random.default_rng(12)
+    nb = 6000
+    b_rows = [np.unique(rng.integers(0, ncols, 40)) for _ in range(nb)]
+    B = HostCSR(nb, ncols,
+                np.concatenate([[0], np.cumsum([len(r) for r in b_rows])]).astype(np.int32),
+                np.concatenate(b_rows).astype(np.int32),
+                rng.uniform(0.1, 1, sum(len(r) for r in b_rows)))
+    cols = [np.arange(nb), np.sort(rng.choice(nb, 1100, replace=False)),
+            np.sort(rng.choice(nb, 40, replace=False)), np.arange(0, nb, 3)]
+    A = HostCSR(len(cols), nb,
+                np.concatenate([[0], np.cumsum([len(c) for c in cols])]).astype(np.int32),
+                np.concatenate(cols).astype(np.int32), rng.uniform(0.1, 1, sum(map(len, cols))))
+    handle.set_option(N.OPT_ONE_PASS, passes)
+    try:
+        C = gpu_product(A, B, handle, np.float64)
+        info = handle.info()
+    finally:
+        handle.set_option(N.OPT_ONE_PASS, 0)
+    assert int(np.diff(C.rpt).max()) > 200_000
+    wide = handle.ladder(1, 8)
+    assert info["num_bin_rows"][len(wide) - 2] == 3      # the three rows past 32,768
+    check(oracle_mod, A, B, C, np.float64, f"wide_cluster_bitmap_{ncols}_pass{passes}",
+          positive=True)
+
+
+def test_rows_past_the_cluster_bitmaps_run_global(handle, oracle_mod):
+    """B of 9 M columns (more than 8 CTAs x 2^20): the cluster bitmap bin hands
+    its rows to the global bitmap bin."""
+    rng = np.random.default_rng(13)
+    nb, ncols = 3000, 9_000_001
+    b_rows = [np.unique(rng.integers(0, ncols, 30)) for _ in range(nb)]
+    B = HostCSR(nb, ncols,
+                np.concatenate([[0], np.cumsum([len(r) for r in b_rows])]).astype(np.int32),
+                np.concatenate(b_rows).astype(np.int32),
+                rng.uniform(0.1, 1, sum(len(r) for r in b_rows)))
+    A = HostCSR(2, nb, np.array([0, nb, nb + 5], np.int32),
+                np.concatenate([np.arange(nb), np.arange(5)]).astype(np.int32),
+                rng.uniform(0.1, 1, nb + 5))
+    C = gpu_product(A, B, handle, np.float64)
+    assert int(np.diff(C.rpt).max()) > 80_000
+    check(oracle_mod, A, B, C, np.float64, "wide_past_cluster_bitmaps", positive=True)
+
+
+@pytest.mark.parametrize("passes", [1, 2])
 def test_high_compression_stencil(handle, oracle_mod, passes):
     """A 27-point stencil squared: ~5.9 products per entry of C, all
     accumulated with global reductions into the row's slice of C.val; in

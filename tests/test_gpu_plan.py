@@ -62,7 +62,10 @@ def test_plan_tuned(handle, oracle_mod):
     p = plan(dA, dA, tune=True, handle=handle)
     try:
         info = p.info()
-        assert len(info["candidates"]) == 6 and 0 <= info["chosen"] < 6
+        # team limits x {1, 0.75, 0.5}, CTA limits x {1, 0.5}, 4 or 8 streams
+        assert len(info["candidates"]) == 12 and 0 <= info["chosen"] < 12
+        assert {(c["team_scale"], c["cta_scale"], c["streams"]) for c in info["candidates"]} == \
+            {(t, c, s) for t in (1.0, 0.75, 0.5) for c in (1.0, 0.5) for s in (4, 8)}
         assert all(c["ms"] > 0 for c in info["candidates"])
         best = info["candidates"][info["chosen"]]["ms"]
         assert best == min(c["ms"] for c in info["candidates"])

@@ -15,14 +15,22 @@ def _server(**kw):
     s.max_batch = kw.get("max_batch", 256)
     s.solo_nip = kw.get("solo_nip", 1000)
     s.batch_nip = kw.get("batch_nip", 5000)
+    s.batch_nip_min = kw.get("batch_nip_min", s.batch_nip)
+    s.batch_cols = kw.get("batch_cols", 1 << 40)
+    s.workers = kw.get("workers", 1)
     s._queue = deque()
     s._in_flight_bytes = 0
     s._cv = threading.Condition()
     return s
 
 
-def _req(rid, nip, bound=None):
-    r = Request(None, None, rid=rid)
+class _Op:
+    def __init__(self, n):
+        self.n = n
+
+
+def _req(rid, nip, bound=None, cols=10):
+    r = Request(None, _Op(cols), rid=rid)
     r.nip = nip
     r.bound_bytes = nip * 12 if bound is None else bound
     return r
@@ -80,3 +88,22 @@ def test_skipped_large_requests_are_restored(n):
                                                                               _req(2, 10)])
     assert _ids(s._admit()[0]) == [0, 1]
     assert _ids(s._queue) == [10 + i for i in range(n)] + [2]
+
+
+def test_batch_cap_follows_the_backlog():
+    # a long queue makes long batches (up to batch_nip), a short one short ones
+    s = _server(batch_nip=1000, batch_nip_min=100, workers=2)
+    s._queue.extend([_req(i, 40) for i in range(100)])      # backlog 4000 -> cap 1000
+    assert len(s._admit()[0]) == 25
+    s = _server(batch_nip=1000, batch_nip_min=100, workers=2)
+    s._queue.extend([_req(i, 40) for i in range(6)])        # backlog 240 -> cap 120
+    assert len(s._admit()[0]) == 3
+
+
+def test_batch_column_cap():
+    s = _server(batch_cols=100)
+    s._queue.extend([_req(i, 10, cols=40) for i in range(5)])
+    assert _ids(s._admit()[0]) == [0, 1]
+    s = _server(batch_cols=100)
+    s._queue.extend([_req(0, 10, cols=500), _req(1, 10, cols=5)])
+    assert _ids(s._admit()[0]) == [0]           # wider than the cap: alone
