@@ -41,7 +41,10 @@ FALLBACK_HBM_GBS = 6650.0
 # 20261203), from an ncu capture of that kernel alone on that product
 # (`-k <kernel> -c 1`, cold caches): key (kernel, value dtype).  Other
 # workloads report traffic null.
-MEASURED_TRAFFIC = {}
+MEASURED_TRAFFIC = {
+    ("s2n_bitmap1024", "f64"): 85_889_536 + 68_849_408,
+    ("esc_cta256_n3072", "f64"): 80_065_280 + 64_517_376,
+}
 
 
 def metric_name(dtype: str) -> str:

@@ -207,21 +207,23 @@ __global__ __launch_bounds__(THREADS) void k_esc_team(ProductArgs p) {
 
 // Expand-sort-compress for rows of up to NMAX products with a whole CTA (the
 // 256-thread bin's range).  As the team version, with an unsigned key
-// (column << SHIFT | q), SHIFT = log2 of the sort capacity, stored with its
-// top bit flipped so that the signed register sort orders it as unsigned
-// (B.n <= 2^(32 - SHIFT)).  Compression: each thread takes a contiguous run
-// of sorted positions, counts the column heads in it, a block scan gives its
-// first output slot, and each head sums its column's run (which may run into
-// the next thread's positions) in product order.
+// (column << SHIFT | q), SHIFT = log2 of the sort capacity (B.n <= 2^(32 -
+// SHIFT)).  The keys are staged in product order and sorted by a stable
+// radix sort of their column bits only (sort.cuh cta_radix_sort: 3 passes
+// for B.n <= 2^21), so a column's products stay in product order.
+// Compression: each thread takes a contiguous run of sorted positions,
+// counts the column heads in it, a block scan gives its first output slot,
+// and each head sums its column's run (which may run into the next thread's
+// positions) in product order.
 template<typename V, int THREADS, int NMAX>
 struct EscCtaLayout {
     static constexpr int P = next_pow2(NMAX);
-    static constexpr int K = P > THREADS * 16 ? P : THREADS * 16;  // sort slots
     static constexpr int SHIFT = ilog2(P);
+    static constexpr int RMAX = (NMAX + THREADS - 1) / THREADS;  // radix rounds per warp
     static constexpr size_t vals_bytes = sizeof(V) * NMAX;
-    static constexpr size_t keys_bytes = sizeof(int32_t) * K;
-    static constexpr size_t bytes = vals_bytes + keys_bytes + sizeof(CtaScratch<THREADS>);
-    static_assert(NMAX <= THREADS * 16, "the register sort takes THREADS * 16 keys");
+    static constexpr size_t keys_bytes = sizeof(uint32_t) * NMAX;
+    static constexpr size_t hist_bytes = sizeof(int32_t) * 128 * (THREADS / kWarp);
+    static constexpr size_t bytes = vals_bytes + keys_bytes + hist_bytes + sizeof(CtaScratch<THREADS>);
     static_assert(bytes <= 232448, "an ESC CTA bin's shared memory exceeds 227 KB");
 };
 
@@ -233,8 +235,10 @@ __global__ __launch_bounds__(THREADS) void k_esc_cta(ProductArgs p) {
     constexpr int NW = THREADS / kWarp;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* vals = reinterpret_cast<V*>(smem_raw);
-    int32_t* keys = reinterpret_cast<int32_t*>(smem_raw + L::vals_bytes);
-    auto& sc = *reinterpret_cast<CtaScratch<THREADS>*>(smem_raw + L::vals_bytes + L::keys_bytes);
+    uint32_t* keys = reinterpret_cast<uint32_t*>(smem_raw + L::vals_bytes);
+    int32_t* hist = reinterpret_cast<int32_t*>(smem_raw + L::vals_bytes + L::keys_bytes);
+    auto& sc = *reinterpret_cast<CtaScratch<THREADS>*>(smem_raw + L::vals_bytes + L::keys_bytes +
+                                                        L::hist_bytes);
     const int tid = threadIdx.x;
     const int row = p.rows[blockIdx.x];
     const int c0 = p.c_rpt[row];
@@ -255,20 +259,20 @@ __global__ __launch_bounds__(THREADS) void k_esc_cta(ProductArgs p) {
                 report(p.status, kStBadInput, row, col);
                 col = 0;
             }
-            const uint32_t u = (static_cast<uint32_t>(col) << SHIFT) | static_cast<uint32_t>(q);
-            keys[q] = static_cast<int32_t>(u ^ 0x80000000u);
+            keys[q] = (static_cast<uint32_t>(col) << SHIFT) | static_cast<uint32_t>(q);
             vals[q] = kp.prod;
         });
-    cta_sort_swz<THREADS>(keys, nip);
-    auto unkey = [&](int i) { return static_cast<uint32_t>(keys[swz(i)]) ^ 0x80000000u; };
+    // the column bits of the keys: B.n - 1 needs this many
+    const int colbits = 32 - __clz(p.n_cols > 1 ? p.n_cols - 1 : 1);
+    cta_radix_sort<THREADS, L::RMAX>(keys, nip, SHIFT, colbits, hist, sc.warp_tot);
     const int per = (nip + THREADS - 1) / THREADS;
     const int i0 = min(tid * per, nip);
     const int i1 = min(i0 + per, nip);
     int heads = 0;
     {
-        uint32_t prev = i0 > 0 ? (unkey(i0 - 1) >> SHIFT) : 0xffffffffu;
+        uint32_t prev = i0 > 0 ? (keys[i0 - 1] >> SHIFT) : 0xffffffffu;
         for (int i = i0; i < i1; i++) {
-            const uint32_t c = unkey(i) >> SHIFT;
+            const uint32_t c = keys[i] >> SHIFT;
             heads += c != prev;
             prev = c;
         }
@@ -278,14 +282,14 @@ __global__ __launch_bounds__(THREADS) void k_esc_cta(ProductArgs p) {
     int r = inc - heads;
     int32_t* out_col = p.c_col + c0;
     V* out_val = static_cast<V*>(p.c_val) + c0;
-    uint32_t prev = i0 > 0 ? (unkey(i0 - 1) >> SHIFT) : 0xffffffffu;
+    uint32_t prev = i0 > 0 ? (keys[i0 - 1] >> SHIFT) : 0xffffffffu;
     for (int i = i0; i < i1; i++) {
-        const uint32_t u = unkey(i);
+        const uint32_t u = keys[i];
         const uint32_t c = u >> SHIFT;
         if (c != prev) {
             V sum = vals[u & QMASK];
             for (int k = i + 1; k < nip; k++) {
-                const uint32_t w = unkey(k);
+                const uint32_t w = keys[k];
                 if ((w >> SHIFT) != c) break;
                 sum += vals[w & QMASK];
             }

@@ -205,4 +205,87 @@ __device__ __forceinline__ void cta_sort_swz(int32_t* keys, int n) {
     }
 }
 
+// Stable CTA radix sort of keys[0, n) by their bits [lo_bit, lo_bit + nbits),
+// in place, 7 bits per pass.  Warp w owns the segment [w S, (w + 1) S),
+// S = 32 ceil(n / THREADS) <= 32 RMAX; in round i lane l holds key
+// w S + 32 i + l, so rounds, then lanes, follow the keys' order.  Per pass:
+// every thread loads its keys into registers (so the pass may scatter over
+// the array it read); each warp ranks its keys per digit -- lanes with the
+// same digit in a round find one another through 7 ballots and the lowest of
+// them adds their count to the warp's counter -- then one block scan over
+// (digit, warp) gives every key its place.  `hist` holds 128 * THREADS / 32
+// ints.  All threads must call it.  Equal digits keep their order, so keys
+// whose low bits hold their input position come out ordered by the sort bits
+// and then by position.
+template<int THREADS, int RMAX>
+__device__ __forceinline__ void cta_radix_sort(uint32_t* keys, int n, int lo_bit, int nbits,
+                                               int32_t* hist, int32_t* warp_tot) {
+    constexpr int NW = THREADS / kWarp;
+    constexpr int DIGITS = 128;
+    static_assert(NW * DIGITS == 4 * THREADS, "four counters per thread in the scan");
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int w = tid >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const int S = kWarp * ((n + THREADS - 1) / THREADS);
+    const int R = S / kWarp;  // <= RMAX
+    int32_t* wh = hist + w * DIGITS;
+    for (int bit = lo_bit; bit < lo_bit + nbits; bit += 7) {
+        uint32_t k[RMAX];
+        int rk[RMAX];
+#pragma unroll
+        for (int i = 0; i < RMAX; i++) {
+            const int idx = w * S + kWarp * i + lane;
+            k[i] = (i < R && idx < n) ? keys[idx] : 0u;
+        }
+#pragma unroll
+        for (int c = 0; c < DIGITS / kWarp; c++) wh[c * kWarp + lane] = 0;
+        __syncthreads();  // every key is in registers; the counters are clear
+#pragma unroll
+        for (int i = 0; i < RMAX; i++) {
+            if (i < R) {
+                const bool valid = w * S + kWarp * i + lane < n;
+                const unsigned d = (k[i] >> bit) & (DIGITS - 1);
+                unsigned peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+                for (int b = 0; b < 7; b++) {
+                    const unsigned m = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+                    peers &= ((d >> b) & 1u) ? m : ~m;
+                }
+                const int pre = wh[d];
+                rk[i] = pre + __popc(peers & lt);
+                __syncwarp();
+                if (valid && (peers & lt) == 0u) wh[d] = pre + __popc(peers);
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // exclusive scan of the counters in (digit, warp) order
+        int v[4];
+        int sum = 0;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int L = 4 * tid + c;
+            v[c] = hist[(L & (NW - 1)) * DIGITS + (L / NW)];
+            sum += v[c];
+        }
+        int run = block_inclusive_scan<THREADS>(sum, warp_tot) - sum;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int L = 4 * tid + c;
+            hist[(L & (NW - 1)) * DIGITS + (L / NW)] = run;
+            run += v[c];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < RMAX; i++) {
+            if (i < R && w * S + kWarp * i + lane < n) {
+                const unsigned d = (k[i] >> bit) & (DIGITS - 1);
+                keys[wh[d] + rk[i]] = k[i];
+            }
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace b200
