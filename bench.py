@@ -81,6 +81,12 @@ def parse():
     ap.add_argument("--no-tune", action="store_true",
                     help="batch mode: plan the batch without the autotuner")
     ap.add_argument("--requests", type=int, default=600)
+    ap.add_argument("--workers", type=int, default=None,
+                    help="served mode: worker threads of the server (default 4)")
+    ap.add_argument("--solo-nip", type=int, default=None,
+                    help="served mode: NIP from which a request runs alone")
+    ap.add_argument("--batch-nip-min", type=int, default=None,
+                    help="served mode: the smallest NIP cap of a batch")
     ap.add_argument("--load", type=float, default=0.8,
                     help="served mode: offered load as a fraction of the plain path's capacity")
     return ap.parse_args()
@@ -378,8 +384,18 @@ def run_ours(args, rank, world, local_rank):
         for k in recs:
             kernel_ms.setdefault((k["phase"], k["bin"], k["name"]), []).append(k["ms"])
     torch.cuda.synchronize()
-    h.set_option(N.OPT_PROFILE, 0)
+    # the same product with its default side streams: each launch's start and
+    # duration after the first launch (the fill bins overlap here)
     h.set_option(N.OPT_STREAMS, nside)
+    timeline = []
+    for i in range(3):
+        flush.fill_(float(i))
+        C = proposal(dA, dA, h)
+        del C
+        timeline = [{"kernel": k["name"], "start_ms": round(k["start_ms"], 4),
+                     "ms": round(k["ms"], 4)} for k in h.profile()]
+    torch.cuda.synchronize()
+    h.set_option(N.OPT_PROFILE, 0)
     launches = launches_per_step * args.steps
 
     value = replica_gflops(nip, args.steps, world, total_ms)
@@ -522,6 +538,7 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": launches,
         "kernels": kernels[:12],
         "serial_kernel_ms_per_step": serial_total,
+        "timeline_concurrent": timeline,
         "host_syncs_per_step": info["host_syncs"],
         "side_streams": nside,
         "host_phase_us_last_step": phase_us,
@@ -749,7 +766,7 @@ def served_pool(seed: int):
     return [[DeviceCSR.from_host(a) for a in pool] for pool in (small, medium, large)]
 
 
-SERVER_WORKERS = 2
+SERVER_WORKERS = 4
 
 
 def run_served(args, local_rank):
@@ -761,6 +778,7 @@ def run_served(args, local_rank):
     from gpuspgemm_b200.serve import SpgemmServer, latency_summary
 
     torch.cuda.set_device(local_rank)
+    workers = args.workers if args.workers is not None else SERVER_WORKERS
     pools = served_pool(args.seed)
     rng = np.random.default_rng(args.seed + 7)
     kinds = rng.choice(3, size=args.requests, p=[0.70, 0.25, 0.05])
@@ -796,7 +814,12 @@ def run_served(args, local_rank):
         return np.array(lat), _t.perf_counter() - t_start
 
     def served(arrivals):
-        server = SpgemmServer(memory_budget=48 << 30, workers=SERVER_WORKERS, device=local_rank)
+        kw = {}
+        if args.solo_nip is not None:
+            kw["solo_nip"] = args.solo_nip
+        if args.batch_nip_min is not None:
+            kw["batch_nip_min"] = args.batch_nip_min
+        server = SpgemmServer(memory_budget=48 << 30, workers=workers, device=local_rank, **kw)
         reqs = []
         t_start = _t.perf_counter()
         for d, ta in zip(picks, arrivals):
@@ -855,7 +878,8 @@ def run_served(args, local_rank):
         "config": {"requests": len(picks), "mix": {k: int((kinds == i).sum()) for i, k in
                                                    enumerate(["small", "medium", "large"])},
                    "nip_total": total_nip, "memory_budget_bytes": 48 << 30,
-                   "workers": SERVER_WORKERS},
+                   "workers": workers, "solo_nip": args.solo_nip,
+                   "batch_nip_min": args.batch_nip_min},
         "saturation": {"served_products_per_s": len(picks) / span_sat,
                        "plain_products_per_s": len(picks) / span_plain_sat,
                        "speedup": span_plain_sat / span_sat,

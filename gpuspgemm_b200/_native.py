@@ -96,6 +96,7 @@ class KernelTime(C.Structure):
         ("bin", C.c_int32),
         ("rows", C.c_int32),
         ("ms", C.c_float),
+        ("start_ms", C.c_float),
     ]
 
 

@@ -92,7 +92,7 @@ class Handle:
         arr = (N.KernelTime * max(cnt.value, 1))()
         N.check(N.lib().spgemm_last_profile(self.ptr, arr, cnt.value, C.byref(cnt)))
         return [{"name": k.name.decode(), "phase": k.phase, "bin": k.bin, "rows": k.rows,
-                 "ms": k.ms} for k in arr[: cnt.value]]
+                 "ms": k.ms, "start_ms": k.start_ms} for k in arr[: cnt.value]]
 
     def ladder(self, which: int, dtype_bytes: int = 8) -> list[int]:
         nb = C.c_int()

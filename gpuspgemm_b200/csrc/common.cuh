@@ -241,16 +241,6 @@ __device__ __forceinline__ int lower_bound_present(const int32_t* cols, int n, i
     return lo;
 }
 
-// Warp-cooperative insert: the lanes of `mask` (converged, every one calling)
-// that hold the same key elect their lowest lane, and only that lane probes
-// the table, so a key repeated across the lanes costs one CAS sequence
-// instead of one per lane contending for the same slot.  Lanes with `valid`
-// false take part in the match only.  Returns 1 on the electing lane when the
-// key was new, else 0 -- the lanes' sum is the number of new keys.
-__device__ __forceinline__ int table_insert_dedup(int32_t* table, uint32_t T, int32_t key,
-                                                  bool valid, unsigned mask, DevStatus* st,
-                                                  int32_t row);
-
 // Insert `key` into a linear-probing table of T slots.  Returns 1 if the key
 // was new, 0 if already present.  The probe loop is bounded by T; if it runs
 // out (table full -- impossible for rows routed by their bound) the status
@@ -266,15 +256,6 @@ __device__ __forceinline__ int table_insert(int32_t* table, uint32_t T, int32_t 
     }
     report(st, kStProbeLimit, row);
     return 0;
-}
-
-__device__ __forceinline__ int table_insert_dedup(int32_t* table, uint32_t T, int32_t key,
-                                                  bool valid, unsigned mask, DevStatus* st,
-                                                  int32_t row) {
-    // kEmpty is never a column index, so lanes without a product group apart
-    const unsigned peers = __match_any_sync(mask, valid ? key : kEmpty);
-    const bool leader = (threadIdx.x & 31u) == static_cast<unsigned>(__ffs(peers) - 1);
-    return (valid && leader) ? table_insert(table, T, key, st, row) : 0;
 }
 
 }  // namespace b200

@@ -37,12 +37,15 @@ struct KeyProduct {
     int32_t key;
     V prod;
 };
-// Products in flight per thread, per walk (measured on the 1M power-law
-// product, serialised per-kernel times): the CTA walks 4 (the 256-thread
-// expand-sort-compress bin 0.285 -> 0.261 ms), the bitmap bin 2 (0.470 ->
-// 0.449 ms; 4 gave 0.456), the 16- and 32-lane teams 2 (0.140 -> 0.124 ms for
-// 32 lanes), the 4- and 8-lane teams 1 (their rows hold few products; 2 and
-// 4 cost registers and took 0.097 -> 0.114 / 0.124 ms for 4 lanes).
+// Products in flight per thread, per walk of the expand-sort-compress and
+// bitmap bins (measured on the 1M power-law product, serialised per-kernel
+// times): the 256-thread bin 4 (0.285 -> 0.261 ms), the bitmap bin 2 (0.470
+// -> 0.449 ms; 4 gave 0.456), the 16- and 32-lane teams 2 (0.140 -> 0.124 ms
+// for 32 lanes), the 4- and 8-lane teams 1 (their rows hold few products; 2
+// and 4 cost registers and took 0.097 -> 0.114 / 0.124 ms for 4 lanes).  The
+// hash bins keep one product per thread: their walks end in a shared-memory
+// CAS or a binary search, and wider walks made the stencil products slower
+// (Galerkin A*P 1.49 -> 1.72 ms, R*AP 1.01 -> 1.12 ms).
 constexpr int kWalkU = 4;
 constexpr int kBitmapWalkU = 2;
 template<int G>
@@ -79,11 +82,9 @@ __global__ __launch_bounds__(THREADS) void k_s2n_team(ProductArgs p) {
     team_sync<G>(mask);
     const int a0 = p.a_rpt[row];
     const int a1 = p.a_rpt[row + 1];
-    team_for_products_mlp<G, team_walk_u<G>(), true>(
-        p.a_col, p.b_rpt, a0, a1, [&](int qb, int, int) { return __ldg(p.b_col + qb); },
-        [&](int32_t key, int, int, int, bool valid) {
-            table_insert_dedup(keys, T, key, valid, mask, p.status, row);
-        });
+    team_for_products<G>(p.a_col, p.b_rpt, a0, a1, [&](int qb, int) {
+        table_insert(keys, T, __ldg(p.b_col + qb), p.status, row);
+    });
     team_sync<G>(mask);
     // sort only the row's keys: compact them to the front, then the register
     // sort leaves them in swizzled order (sort.cuh)
@@ -102,14 +103,11 @@ __global__ __launch_bounds__(THREADS) void k_s2n_team(ProductArgs p) {
         out[i] = V(0);
     }
     team_sync<G>(mask);
-    team_for_products_mlp<G, team_walk_u<G>()>(
-        p.a_col, p.b_rpt, a0, a1,
-        [&](int qb, int ai, int) {
-            return KeyProduct<V>{__ldg(p.b_col + qb), ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb)};
-        },
-        [&](const KeyProduct<V>& kp, int, int, int) {
-            atomicAdd(out + lower_bound_present_swz(keys, nnz, kp.key), kp.prod);
-        });
+    team_for_products<G>(p.a_col, p.b_rpt, a0, a1, [&](int qb, int ai) {
+        const int32_t key = __ldg(p.b_col + qb);
+        const int pos = lower_bound_present_swz(keys, nnz, key);
+        atomicAdd(out + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
+    });
 }
 
 // Expand-sort-compress fill of rows with at most NMAX products, for the
@@ -423,11 +421,9 @@ __global__ __launch_bounds__(THREADS) void k_s2n_cta(ProductArgs p) {
     __syncthreads();
     const int a0 = p.a_rpt[row];
     const int a1 = p.a_rpt[row + 1];
-    cta_for_products_mlp<THREADS, kWalkU, true>(
-        p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int, int) { return __ldg(p.b_col + qb); },
-        [&](int32_t key, int, int, int, bool valid) {
-            table_insert_dedup(keys, T, key, valid, 0xffffffffu, p.status, row);
-        });
+    cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int) {
+        table_insert(keys, T, __ldg(p.b_col + qb), p.status, row);
+    });
     const int cnt = cta_compact<THREADS>(keys, T, sc.warp_tot);
     int nnz = bound;
     if (p.row_nnz != nullptr) {  // one-pass: the count is the row's nnz
@@ -447,14 +443,11 @@ __global__ __launch_bounds__(THREADS) void k_s2n_cta(ProductArgs p) {
         out[i] = V(0);
     }
     __syncthreads();
-    cta_for_products_mlp<THREADS, kWalkU>(
-        p.a_col, p.b_rpt, a0, a1, sc,
-        [&](int qb, int ai, int) {
-            return KeyProduct<V>{__ldg(p.b_col + qb), ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb)};
-        },
-        [&](const KeyProduct<V>& kp, int, int, int) {
-            atomicAdd(out + lower_bound_present_swz(keys, nnz, kp.key), kp.prod);
-        });
+    cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int ai) {
+        const int32_t key = __ldg(p.b_col + qb);
+        const int pos = lower_bound_present_swz(keys, nnz, key);
+        atomicAdd(out + pos, ldv<V>(p.a_val, ai) * ldv<V>(p.b_val, qb));
+    });
 }
 
 // Bitmap bin (B.n <= kBitmapCols): the row's hash table is the identity hash

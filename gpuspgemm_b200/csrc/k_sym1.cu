@@ -39,11 +39,9 @@ __global__ __launch_bounds__(THREADS) void k_sym1_team(ProductArgs p) {
     const int a0 = p.a_rpt[row];
     const int a1 = p.a_rpt[row + 1];
     int cnt = 0;
-    team_for_products_mlp<G, (G >= 16 ? 2 : 1), true>(
-        p.a_col, p.b_rpt, a0, a1, [&](int qb, int, int) { return __ldg(p.b_col + qb); },
-        [&](int32_t key, int, int, int, bool valid) {
-            cnt += table_insert_dedup(table, T, key, valid, mask, p.status, row);
-        });
+    team_for_products<G>(p.a_col, p.b_rpt, a0, a1, [&](int qb, int) {
+        cnt += table_insert(table, T, __ldg(p.b_col + qb), p.status, row);
+    });
     cnt = team_sum<G>(mask, cnt);
     if (lane == 0) p.c_rpt[row] = cnt;
 }
@@ -58,11 +56,9 @@ __global__ __launch_bounds__(THREADS) void k_sym1_cta(ProductArgs p) {
     const int a0 = p.a_rpt[row];
     const int a1 = p.a_rpt[row + 1];
     int cnt = 0;
-    cta_for_products_mlp<THREADS, 4, true>(
-        p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int, int) { return __ldg(p.b_col + qb); },
-        [&](int32_t key, int, int, int, bool valid) {
-            cnt += table_insert_dedup(smem, T, key, valid, 0xffffffffu, p.status, row);
-        });
+    cta_for_products<THREADS>(p.a_col, p.b_rpt, a0, a1, sc, [&](int qb, int) {
+        cnt += table_insert(smem, T, __ldg(p.b_col + qb), p.status, row);
+    });
     cnt = block_sum<THREADS>(cnt, sc.warp_tot);
     if (threadIdx.x == 0) p.c_rpt[row] = cnt;
 }
@@ -137,6 +133,7 @@ __global__ __launch_bounds__(THREADS) void k_sym1_cluster(ProductArgs p) {
         const int end = min(base + THREADS, a1);
         if (__syncthreads_or(ops.spilled() ? 1 : 0)) break;
         // lanes holding the same key elect one lane to probe the remote table
+        // (each probe is a CAS in another CTA's shared memory)
         cta_for_products_mlp<THREADS, 2, true>(
             p.a_col, p.b_rpt, base, end, sc, [&](int qb, int, int) { return __ldg(p.b_col + qb); },
             [&](int32_t key, int, int, int, bool valid) {

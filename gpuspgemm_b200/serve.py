@@ -76,13 +76,12 @@ class SpgemmServer:
                    (saturation) makes long batches, which amortise each
                    product's fixed cost over many requests.
     batch_cols:    most columns of a packed batch's B (the sum of its
-                   members' B.n): up to 2^20 the batch runs the bitmap and
-                   expand-sort-compress fill bins.
+                   members' B.n).
     size_chunk:    most arrivals a worker sizes in one call before it tries to
                    admit.
     """
 
-    def __init__(self, memory_budget: int = 32 << 30, max_batch: int = 256, workers: int = 2,
+    def __init__(self, memory_budget: int = 32 << 30, max_batch: int = 256, workers: int = 4,
                  device: int = 0, solo_nip: int = 4 << 20, batch_nip: int = 32 << 20,
                  batch_nip_min: int = 4 << 20, batch_cols: int = 1 << 20,
                  size_chunk: int = 256):

@@ -222,6 +222,8 @@ typedef struct spgemm_kernel_time {
     int32_t bin;    /* ladder bin, -1 for binning kernels */
     int32_t rows;   /* rows the launch handled (-1 if only known on the device) */
     float ms;       /* event-timed duration */
+    float start_ms; /* launch start after the call's first launch (a timeline when
+                       launches run side by side on the handle's side streams) */
 } spgemm_kernel_time;
 
 SPGEMM_API spgemm_status spgemm_last_profile(spgemm_handle_t handle, spgemm_kernel_time* out,

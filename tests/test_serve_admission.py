@@ -107,3 +107,4 @@ def test_batch_column_cap():
     s = _server(batch_cols=100)
     s._queue.extend([_req(0, 10, cols=500), _req(1, 10, cols=5)])
     assert _ids(s._admit()[0]) == [0]           # wider than the cap: alone
+
