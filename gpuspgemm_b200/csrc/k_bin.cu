@@ -37,8 +37,8 @@ __device__ __forceinline__ long long warp_sum_ll(long long v) {
 __global__ __launch_bounds__(kBinThreads) void k_nip_hist(
     const int32_t* __restrict__ a_rpt, const int32_t* __restrict__ a_col,
     const int32_t* __restrict__ b_rpt, int32_t m, int32_t* __restrict__ c_rpt,
-    int32_t* __restrict__ hist, Plan* __restrict__ plan, DevStatus* __restrict__ st,
-    const __grid_constant__ Ladder lad) {
+    int32_t* __restrict__ nip_copy, int32_t* __restrict__ hist, Plan* __restrict__ plan,
+    DevStatus* __restrict__ st, const __grid_constant__ Ladder lad) {
     __shared__ int32_t s_hist[kMaxBins];
     __shared__ long long s_tot[kBinThreads / kWarp];
     __shared__ int32_t s_max[kBinThreads / kWarp];
@@ -103,6 +103,7 @@ __global__ __launch_bounds__(kBinThreads) void k_nip_hist(
                 key = static_cast<int32_t>(nip);
             }
             c_rpt[r] = key;
+            if (nip_copy != nullptr) nip_copy[r] = key;
             my_tot += nip;
             my_max = max(my_max, key);
             if (key > 0) atomicAdd(&s_hist[find_bin(lad, key)], 1);
@@ -422,11 +423,12 @@ __global__ void k_total_nip(const int32_t* __restrict__ a_rpt, const int32_t* __
 }  // namespace
 
 cudaError_t launch_nip_hist(const int32_t* a_rpt, const int32_t* a_col, const int32_t* b_rpt,
-                            int32_t m, int32_t* c_rpt, int32_t* hist, Plan* plan,
-                            DevStatus* st, const Ladder& lad, cudaStream_t s) {
+                            int32_t m, int32_t* c_rpt, int32_t* nip_copy, int32_t* hist,
+                            Plan* plan, DevStatus* st, const Ladder& lad, cudaStream_t s) {
     const int g = bin_ctas(m);
     if (g == 0) return cudaSuccess;
-    k_nip_hist<<<g, kBinThreads, 0, s>>>(a_rpt, a_col, b_rpt, m, c_rpt, hist, plan, st, lad);
+    k_nip_hist<<<g, kBinThreads, 0, s>>>(a_rpt, a_col, b_rpt, m, c_rpt, nip_copy, hist, plan, st,
+                                         lad);
     return cudaGetLastError();
 }
 

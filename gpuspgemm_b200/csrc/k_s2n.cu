@@ -880,48 +880,55 @@ cudaError_t launch_cta(const ProductArgs& p, cudaStream_t s) {
 }
 
 // Order a bin's row list by slot size (the row's NIP in one-pass mode, its
-// nnz in two), largest first, ties by row: one CTA, a bitonic sort of
-// (INT32_MAX - size) << 32 | row keys in shared memory.  With the persistent
-// bins taking rows from a counter, the CTAs then finish together (largest
-// first: each CTA's last row is a short one).
+// nnz in two), largest first: one CTA, a counting sort by size bucket (size /
+// 32, capped), buckets in descending order, rows in a bucket in any order.
+// With the persistent bins taking rows from a counter, the CTAs then finish
+// together (largest first: each CTA's last row is a short one).  The kernel
+// also zeroes the bin's row counter for the launch that follows.
 constexpr int kSortRowsMax = 8192;
 constexpr int kSortThreads = 1024;
+constexpr int kSizeBuckets = 2048;
 
 __global__ __launch_bounds__(kSortThreads) void k_rows_largest_first(int32_t* __restrict__ rows,
                                                                      int32_t n,
-                                                                     const int32_t* __restrict__ c_rpt) {
-    extern __shared__ unsigned long long s_key[];
-    int N = 1;
-    while (N < n) N <<= 1;
-    for (int i = threadIdx.x; i < N; i += kSortThreads) {
-        unsigned long long k = ~0ull;
-        if (i < n) {
-            const int r = rows[i];
-            const int size = c_rpt[r + 1] - c_rpt[r];
-            k = (static_cast<unsigned long long>(static_cast<uint32_t>(INT32_MAX - size)) << 32) |
-                static_cast<uint32_t>(r);
-        }
-        s_key[i] = k;
+                                                                     const int32_t* __restrict__ c_rpt,
+                                                                     int32_t* __restrict__ work) {
+    constexpr int PER = kSizeBuckets / kSortThreads;
+    __shared__ int32_t s_count[kSizeBuckets];  // per bucket: count, then first slot
+    __shared__ int32_t s_out[kSortRowsMax];
+    __shared__ int32_t s_warp[kSortThreads / kWarp];
+    const int tid = threadIdx.x;
+    if (tid == 0) *work = 0;
+    for (int i = tid; i < kSizeBuckets; i += kSortThreads) s_count[i] = 0;
+    __syncthreads();
+    // descending: bucket 0 holds the largest rows
+    auto bucket = [&](int r) {
+        const int size = c_rpt[r + 1] - c_rpt[r];
+        return kSizeBuckets - 1 - min(size >> 5, kSizeBuckets - 1);
+    };
+    for (int i = tid; i < n; i += kSortThreads) atomicAdd(&s_count[bucket(rows[i])], 1);
+    __syncthreads();
+    // exclusive scan of the bucket counts: PER consecutive buckets a thread
+    int v[PER];
+    int sum = 0;
+#pragma unroll
+    for (int c = 0; c < PER; c++) {
+        v[c] = s_count[tid * PER + c];
+        sum += v[c];
+    }
+    int run = block_inclusive_scan<kSortThreads>(sum, s_warp) - sum;
+#pragma unroll
+    for (int c = 0; c < PER; c++) {
+        s_count[tid * PER + c] = run;
+        run += v[c];
     }
     __syncthreads();
-    for (int k = 2; k <= N; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < (N >> 1); i += kSortThreads) {
-                const int lo = 2 * i - (i & (j - 1));
-                const int hi = lo + j;
-                const bool up = (lo & k) == 0;
-                const unsigned long long a = s_key[lo];
-                const unsigned long long b = s_key[hi];
-                if ((a > b) == up) {
-                    s_key[lo] = b;
-                    s_key[hi] = a;
-                }
-            }
-            __syncthreads();
-        }
+    for (int i = tid; i < n; i += kSortThreads) {
+        const int r = rows[i];
+        s_out[atomicAdd(&s_count[bucket(r)], 1)] = r;
     }
-    for (int i = threadIdx.x; i < n; i += kSortThreads)
-        rows[i] = static_cast<int32_t>(s_key[i] & 0xffffffffull);
+    __syncthreads();
+    for (int i = tid; i < n; i += kSortThreads) rows[i] = s_out[i];
 }
 
 template<typename V, int THREADS, int CAP>
@@ -931,14 +938,16 @@ cudaError_t launch_bitmap(const ProductArgs& p, cudaStream_t s) {
     const int sms = p.sm_count > 0 ? p.sm_count : 148;
     const int grid = p.nrows < sms ? p.nrows : sms;
     if (p.work != nullptr) {
-        // the bin's row list is the library's own (a binning pass wrote it)
+        // the bin's row list is the library's own (a binning pass wrote it);
+        // the sort kernel also zeroes the row counter
         if (p.nrows > grid && p.nrows <= kSortRowsMax) {
-            k_rows_largest_first<<<1, kSortThreads, sizeof(unsigned long long) * kSortRowsMax, s>>>(
-                const_cast<int32_t*>(p.rows), p.nrows, p.c_rpt);
+            k_rows_largest_first<<<1, kSortThreads, 0, s>>>(const_cast<int32_t*>(p.rows),
+                                                            p.nrows, p.c_rpt, p.work);
             if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return e;
-        }
-        if (cudaError_t e = cudaMemsetAsync(p.work, 0, sizeof(int32_t), s); e != cudaSuccess)
+        } else if (cudaError_t e = cudaMemsetAsync(p.work, 0, sizeof(int32_t), s);
+                   e != cudaSuccess) {
             return e;
+        }
     }
     k_s2n_bitmap<V, THREADS, CAP><<<grid, THREADS, BitmapLayout<V, THREADS, CAP>::bytes, s>>>(p);
     return cudaGetLastError();
@@ -1076,6 +1085,19 @@ B200_S2N_ESC_LADDER(double)
 B200_S2N_ESC_LADDER(float)
 #undef B200_S2N_ESC_LADDER
 
+// The 32-lane expand-sort-compress bin for rows of at most kEscSplit products,
+// launched when the device-side decision moved the 32-lane / 256-thread split
+// to kEscSplit: half the shared memory of the 768-product kernel per team, so
+// twice the CTAs per SM (ncu: the 768-product kernel ran 17 % warps active).
+template<typename V>
+struct EscSplitBin {
+    static const BinLauncher entry;
+};
+template<typename V>
+const BinLauncher EscSplitBin<V>::entry = {BinKind::Team, kEscSplit, 8, 256,
+                                           EscLayout<V, 32, 256, kEscSplit>::bytes,
+                                           "esc_team32_n512", launch_esc<V, 32, 256, kEscSplit>};
+
 template<typename V>
 cudaError_t prepare_one() {
     cudaError_t e = cudaSuccess;
@@ -1096,6 +1118,7 @@ cudaError_t prepare_one() {
     B200_SMEM((k_esc_team<V, 8, 256, 48>), (EscLayout<V, 8, 256, 48>::bytes));
     B200_SMEM((k_esc_team<V, 16, 256, 192>), (EscLayout<V, 16, 256, 192>::bytes));
     B200_SMEM((k_esc_team<V, 32, 256, 768>), (EscLayout<V, 32, 256, 768>::bytes));
+    B200_SMEM((k_esc_team<V, 32, 256, kEscSplit>), (EscLayout<V, 32, 256, kEscSplit>::bytes));
     B200_SMEM((k_esc_cta<V, 256, 3072>), (EscCtaLayout<V, 256, 3072>::bytes));
 #undef B200_SMEM
     return e;
@@ -1133,6 +1156,9 @@ int s2n_esc_ladder_f32(const BinLauncher** out) {
     return S2nEscLadder<float>::count;
 }
 
+const BinLauncher* s2n_esc_split_bin_f64() { return &EscSplitBin<double>::entry; }
+const BinLauncher* s2n_esc_split_bin_f32() { return &EscSplitBin<float>::entry; }
+
 cudaError_t launch_esc_sample(const ProductArgs& p, int32_t m, int32_t samples,
                               const EscLimits& lim, EscSample* out, cudaStream_t s) {
     if (samples <= 0) return cudaSuccess;
@@ -1162,10 +1188,7 @@ cudaError_t launch_esc_decide(EscSample* sample, const Ladder& base, int esc_mod
 }
 
 cudaError_t s2n_prepare() {
-    cudaError_t e = cudaFuncSetAttribute(k_rows_largest_first,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(sizeof(unsigned long long) * kSortRowsMax));
-    if (e == cudaSuccess) e = prepare_one<double>();
+    cudaError_t e = prepare_one<double>();
     if (e == cudaSuccess) e = prepare_one<float>();
     return e;
 }

@@ -103,6 +103,10 @@ int s2n_bitmap_ladder_f32(const BinLauncher** out);
 // bitmap and global bins.  Same bin count and limits as the bitmap ladder.
 int s2n_esc_ladder_f64(const BinLauncher** out);
 int s2n_esc_ladder_f32(const BinLauncher** out);
+// The one-pass ladder's largest team bin when its split is kEscSplit
+// (rows of at most kEscSplit products: a smaller kernel, more CTAs per SM).
+const BinLauncher* s2n_esc_split_bin_f64();
+const BinLauncher* s2n_esc_split_bin_f32();
 
 // Sampled compression of the first kEscBins fill bins of a one-pass product:
 // the NIP and exact nnz of up to `samples` rows spread evenly over A, summed
@@ -161,11 +165,11 @@ constexpr int kBinRowsPerCta = 1024;
 
 inline int bin_ctas(int32_t m) { return (m + kBinRowsPerCta - 1) / kBinRowsPerCta; }
 
-// Pass 1 (key = NIP): writes nip[r] into c_rpt[r], per-CTA bin histograms and
-// the plan's total / max.
+// Pass 1 (key = NIP): writes nip[r] into c_rpt[r] (and nip_copy[r] when not
+// nullptr), per-CTA bin histograms and the plan's total / max.
 cudaError_t launch_nip_hist(const int32_t* a_rpt, const int32_t* a_col, const int32_t* b_rpt,
-                            int32_t m, int32_t* c_rpt, int32_t* hist, Plan* plan,
-                            DevStatus* st, const Ladder& lad, cudaStream_t s);
+                            int32_t m, int32_t* c_rpt, int32_t* nip_copy, int32_t* hist,
+                            Plan* plan, DevStatus* st, const Ladder& lad, cudaStream_t s);
 // Pass 1' (key = nnz already in c_rpt): per-CTA sums and bin histograms.
 // dlad: limits chosen on the device (same bin count as lad), or nullptr.
 cudaError_t launch_nnz_hist(const int32_t* c_rpt, int32_t m, int32_t* hist, int64_t* cta_sum,

@@ -48,6 +48,9 @@ spgemm_status cuda_fail(cudaError_t e, const char* what) {
     } while (0)
 
 constexpr int kMaxSide = 8;
+// Bytes of the scratch front (status, plans, fail counter, sample, ladder)
+// that one synchronisation copies back.
+constexpr size_t kFrontBytes = 4096;
 // Bitmap pool budget of the global bins (bytes).
 constexpr int64_t kBitmapBudget = int64_t(1) << 30;
 
@@ -111,6 +114,7 @@ struct spgemm_handle_s {
     void* slots = nullptr;  // one-pass NIP slot starts (m + 1), grown like the rest
     size_t slots_bytes = 0;
     b200::HostMirror* mirror = nullptr;  // pinned
+    char* front_host = nullptr;          // pinned copy of the scratch front
     // host-operand staging on the device
     void* in_buf = nullptr;
     size_t in_bytes = 0;
@@ -287,23 +291,26 @@ spgemm_status status_to_error(const DevStatus& st) {
     return fail(SPGEMM_ERR_INTERNAL, buf);
 }
 
+// The status word, both plans, the fail counter and the sample sit at the
+// front of the handle's scratch (ensure_scratch): one copy brings them all
+// back, and the host picks the words it asked for out of it.
 spgemm_status sync_mirror(spgemm_handle_s* h, cudaStream_t stream, const Plan* plan,
                           const Scratch& s, bool with_sample = false,
                           const Plan* plan_b = nullptr) {
-    if (plan_b != nullptr)
-        B200_TRY(cudaMemcpyAsync(&h->mirror->plan_b, plan_b, sizeof(Plan), cudaMemcpyDeviceToHost,
-                                 stream));
-    if (with_sample)
-        B200_TRY(cudaMemcpyAsync(&h->mirror->sample, s.sample, sizeof(EscSample),
-                                 cudaMemcpyDeviceToHost, stream));
-    B200_TRY(cudaMemcpyAsync(&h->mirror->plan, plan, sizeof(Plan), cudaMemcpyDeviceToHost,
-                             stream));
-    B200_TRY(cudaMemcpyAsync(&h->mirror->status, s.status, sizeof(DevStatus),
-                             cudaMemcpyDeviceToHost, stream));
-    B200_TRY(cudaMemcpyAsync(&h->mirror->fail_count, s.fail_count, sizeof(int32_t),
-                             cudaMemcpyDeviceToHost, stream));
+    const char* dev0 = static_cast<const char*>(h->scratch);
+    const size_t front = static_cast<size_t>(reinterpret_cast<const char*>(s.hist1) - dev0);
+    if (front > kFrontBytes) return fail(SPGEMM_ERR_INTERNAL, "scratch front exceeds its mirror");
+    B200_TRY(cudaMemcpyAsync(h->front_host, h->scratch, front, cudaMemcpyDeviceToHost, stream));
     B200_TRY(cudaStreamSynchronize(stream));
     h->info.host_syncs++;
+    auto at = [&](const void* dev) {
+        return h->front_host + (static_cast<const char*>(dev) - dev0);
+    };
+    std::memcpy(&h->mirror->plan, at(plan), sizeof(Plan));
+    if (plan_b != nullptr) std::memcpy(&h->mirror->plan_b, at(plan_b), sizeof(Plan));
+    if (with_sample) std::memcpy(&h->mirror->sample, at(s.sample), sizeof(EscSample));
+    std::memcpy(&h->mirror->status, at(s.status), sizeof(DevStatus));
+    std::memcpy(&h->mirror->fail_count, at(s.fail_count), sizeof(int32_t));
     return SPGEMM_OK;
 }
 
@@ -543,9 +550,7 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         ps.b_rpt = B->rpt;
         ps.b_col = B->col;
         ps.status = s.status;
-        if (cudaError_t e = cudaMemsetAsync(s.sample, 0, sizeof(EscSample), stream);
-            e != cudaSuccess)
-            return bail(cuda_fail(e, "reset the compression sample"));
+        // (the sample's sums were zeroed with the scratch front above)
         if (cudaError_t e = cudaEventRecord(h->ev_fork, stream); e != cudaSuccess)
             return bail(cuda_fail(e, "fork the sample stream"));
         if (cudaError_t e = cudaStreamWaitEvent(side, h->ev_fork, 0); e != cudaSuccess)
@@ -559,22 +564,38 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         if (cudaError_t e = cudaEventRecord(h->ev_sample, side); e != cudaSuccess)
             return bail(cuda_fail(e, "join the sample stream"));
     }
+    // A product likely to run one pass is binned for the fill right away and
+    // decided at the one synchronisation that follows; the count binning then
+    // runs only if it turns out two-pass.  Its fill binning scans a copy of
+    // the NIP per row, which the NIP pass writes beside C.rpt.
+    const bool early = cr == nullptr && h->one_pass != 2 &&
+                       (h->one_pass == 1 || A->nnz >= kEarlyOnePassNnz);
+    int32_t* off = nullptr;  // the one-pass NIP slots: a scan of the NIP per row
+    bool off_written = false;
+    if (early) {
+        B200_STEP(regrow(h, &h->slots, &h->slots_bytes, sizeof(int32_t) * (size_t(m) + 1),
+                         stream));
+        off = static_cast<int32_t*>(h->slots);
+        off_written = true;
+    }
     B200_STEP(timed(h, "nip_hist", 0, -1, m, stream, [&](cudaStream_t ss) {
-        return launch_nip_hist(A->rpt, A->col, B->rpt, m, c_rpt, s.hist1, s.plan1, s.status,
+        return launch_nip_hist(A->rpt, A->col, B->rpt, m, c_rpt, off, s.hist1, s.plan1, s.status,
                                lad1, ss);
     }));
     // The fill binning by NIP (the one-pass path's), with limits decided on
     // the device when the sample ran: off = the scan of the NIP per row.
-    int32_t* off = nullptr;
     Ladder ladh = ladf;
     if (esc_mode == 1) ladh.limit[kEscBins - 1] = kEscSplit;
     const Ladder* dlad = sampled ? s.dladder : nullptr;
     auto fill_binning = [&]() -> spgemm_status {
-        B200_STEP_R(regrow(h, &h->slots, &h->slots_bytes, sizeof(int32_t) * (size_t(m) + 1),
-                           stream));
-        off = static_cast<int32_t*>(h->slots);
-        B200_TRY(cudaMemcpyAsync(off, c_rpt, sizeof(int32_t) * size_t(m), cudaMemcpyDeviceToDevice,
-                                 stream));
+        if (!off_written) {
+            B200_STEP_R(regrow(h, &h->slots, &h->slots_bytes, sizeof(int32_t) * (size_t(m) + 1),
+                               stream));
+            off = static_cast<int32_t*>(h->slots);
+            B200_TRY(cudaMemcpyAsync(off, c_rpt, sizeof(int32_t) * size_t(m),
+                                     cudaMemcpyDeviceToDevice, stream));
+            off_written = true;
+        }
         if (sampled) B200_TRY(cudaStreamWaitEvent(stream, h->ev_sample, 0));
         B200_STEP_R(timed(h, "nip_fill_hist", 2, -1, m, stream, [&](cudaStream_t ss) {
             return launch_nnz_hist(off, m, s.hist2, s.cta_sum, s.plan2, ladh, ss, dlad);
@@ -599,11 +620,6 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         }));
         return SPGEMM_OK;
     };
-    // A product likely to run one pass is binned for the fill right away and
-    // decided at the one synchronisation that follows; the count binning then
-    // runs only if it turns out two-pass.
-    const bool early = cr == nullptr && h->one_pass != 2 &&
-                       (h->one_pass == 1 || A->nnz >= kEarlyOnePassNnz);
     if (early) {
         B200_STEP(fill_binning());
     } else {
@@ -717,9 +733,9 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
             tmp_col = reinterpret_cast<int32_t*>(base);
             tmp_val = base + o_val;
         }
-        // C.rpt receives each row's exact nnz (rows without products stay 0)
-        B200_ONE_CUDA(cudaMemsetAsync(c_rpt, 0, sizeof(int32_t) * (size_t(m) + 1), stream),
-                      "memset row counts");
+        // C.rpt receives each row's exact nnz from the fill kernel of its bin;
+        // a row without products keeps the NIP of 0 the NIP pass wrote there
+        // (and the scan writes C.rpt[m])
         if (esc_ok) {
             const BinLauncher* esc = nullptr;
             const int nesc = sizeof(V) == 8 ? s2n_esc_ladder_f64(&esc) : s2n_esc_ladder_f32(&esc);
@@ -735,6 +751,10 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
                                                 kEscMaxRatio[b] * static_cast<double>(es.nnz[b])));
                 if (use) {
                     one_fil[b] = esc[b];
+                    // split: the largest team bin holds rows of <= kEscSplit products
+                    if (b == kEscBins - 1 && split)
+                        one_fil[b] = sizeof(V) == 8 ? *s2n_esc_split_bin_f64()
+                                                    : *s2n_esc_split_bin_f32();
                     h->info.esc_mask |= 1 << b;
                 }
             }
@@ -1853,6 +1873,7 @@ spgemm_status spgemm_create(spgemm_handle_t* handle, int device) {
     B200_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     B200_TRY(cudaEventCreateWithFlags(&h->ev_sample, cudaEventDisableTiming));
     B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&h->mirror), sizeof(HostMirror)));
+    B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&h->front_host), kFrontBytes));
     if (spgemm_status st = device_pool(dev, &h->pool); st != SPGEMM_OK) return st;
     *handle = h;
     return SPGEMM_OK;
@@ -1874,6 +1895,7 @@ spgemm_status spgemm_destroy(spgemm_handle_t h) {
     if (h->slots) cudaFree(h->slots);
     if (h->in_buf) cudaFree(h->in_buf);
     if (h->mirror) cudaFreeHost(h->mirror);
+    if (h->front_host) cudaFreeHost(h->front_host);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     // the pool is shared and outlives handles (results may outlive them too);
     // the last handle on the device gives its unused cached memory back
