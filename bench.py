@@ -42,8 +42,8 @@ FALLBACK_HBM_GBS = 6650.0
 # (`-k <kernel> -c 1`, cold caches): key (kernel, value dtype).  Other
 # workloads report traffic null.
 MEASURED_TRAFFIC = {
-    ("s2n_bitmap1024", "f64"): 85_889_536 + 68_849_408,
-    ("esc_cta256_n3072", "f64"): 80_065_280 + 64_517_376,
+    ("s2n_bitmap1024", "f64"): 85_622_272 + 69_268_480,
+    ("esc_cta256_n3072", "f64"): 80_557_824 + 65_419_264,
 }
 
 
