@@ -233,6 +233,183 @@ __global__ __launch_bounds__(THREADS) void k_esc_team(ProductArgs p) {
     if (lane == 0) p.row_nnz[row] = written;
 }
 
+// Expand-sort-compress of the smallest rows (the first one-pass bin) with
+// whole warps over many rows.  A team of G lanes per row leaves most lanes
+// idle there: the 1M power-law product has 826 k rows of 1-12 products, 2.9 on
+// average (ncu: 9 of 32 lanes active per instruction with 4-lane teams).  A
+// warp takes 32 rows of the bin's list and packs them, in list order, into
+// batches of at most 32 products, one per lane.  Per batch:
+//   1. the batch's A entries, flattened over its rows, 32 at a time: each lane
+//      finds its entry's row by a search over the rows' A-entry prefix (held
+//      one per lane), loads the entry and its B row's extent, and a warp scan
+//      of the B-row lengths places each entry's first product;
+//   2. each lane finds its product's entry by a search over that scan, loads
+//      B's column and value, and stages the key (row in the batch << 25 |
+//      column << 5 | product) and the product a_ik * b_kj in shared memory;
+//   3. a warp bitonic sort of the 32 keys orders them by row, column and
+//      product; the first lane of each (row, column) run sums the run in
+//      product order (Gustavson's order, as the team kernels) and writes the
+//      column and sum at its rank in the row; the last lane of each row
+//      writes the row's nnz.
+// Single-entry rows take the same path.  Needs B.n <= 2^20 (the ladder that
+// holds it) and the one-pass mode's NIP-sized slots; a row of more than 32
+// products is reported.
+constexpr int kEscWarpThreads = 256;
+
+template<typename V, int THREADS>
+__global__ __launch_bounds__(THREADS) void k_esc_warp(ProductArgs p) {
+    constexpr int NW = THREADS / kWarp;
+    constexpr unsigned kFull = 0xffffffffu;
+    __shared__ uint32_t s_key[NW][kWarp];
+    __shared__ uint32_t s_sorted[NW][kWarp];
+    __shared__ V s_val[NW][kWarp];
+    const int lane = static_cast<int>(threadIdx.x & 31u);
+    const int w = static_cast<int>(threadIdx.x >> 5);
+    const int r0 = (blockIdx.x * NW + w) * kWarp;
+    if (r0 >= p.nrows) return;  // uniform over the warp
+    const int nr = min(kWarp, p.nrows - r0);
+    // lane j holds row j of the warp's rows
+    int row = 0;
+    int c0 = 0;
+    int nip = 0;
+    int a0 = 0;
+    int deg = 0;
+    if (lane < nr) {
+        row = p.rows[r0 + lane];
+        c0 = p.c_rpt[row];
+        nip = p.c_rpt[row + 1] - c0;  // the row's NIP-sized slot
+        a0 = p.a_rpt[row];
+        deg = p.a_rpt[row + 1] - a0;
+        if (nip > kWarp || nip < 0 || p.row_nnz == nullptr) {
+            report(p.status, kStCapacity, row, nip);
+            nip = 0;  // left out; the status fails the product
+            deg = 0;
+        } else if (nip == 0) {
+            p.row_nnz[row] = 0;
+            deg = 0;  // entries whose B rows are all empty make no product
+        }
+    }
+    const int pin = team_inclusive_scan<kWarp>(kFull, nip, lane);  // products through row lane
+    const int din = team_inclusive_scan<kWarp>(kFull, deg, lane);  // A entries through row lane
+    uint32_t* keys = s_key[w];
+    uint32_t* sorted = s_sorted[w];
+    V* vals = s_val[w];
+    for (int j0 = 0; j0 < nr;) {  // uniform over the warp
+        const int pbase = j0 > 0 ? __shfl_sync(kFull, pin, j0 - 1) : 0;
+        const int dbase = j0 > 0 ? __shfl_sync(kFull, din, j0 - 1) : 0;
+        // rows [j0, j1): the longest run from j0 whose products fit 32 (row j0
+        // always does; pin is non-decreasing, so the run is contiguous)
+        const unsigned take = __ballot_sync(kFull, lane >= j0 && lane < nr && pin - pbase <= kWarp);
+        const int j1 = 32 - __clz(take);
+        const int total = __shfl_sync(kFull, pin, j1 - 1) - pbase;
+        const int dtotal = __shfl_sync(kFull, din, j1 - 1) - dbase;
+        const int drel = din - dbase;  // A entries of rows [j0, lane] (row lanes)
+        int done = 0;                  // products staged
+        for (int f0 = 0; f0 < dtotal; f0 += kWarp) {  // uniform over the warp
+            const int f = f0 + lane;
+            // entry f's row: the first row lane with drel > f (the last with
+            // drel <= f, plus one); for f < dtotal that lane is below j1 - 1
+            int jr = j0 - 1;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+                const int c = jr + step;
+                const int v = __shfl_sync(kFull, drel, c & 31);
+                if (c < j1 && v <= f) jr = c;
+            }
+            jr += 1;
+            const int src = jr & 31;
+            const int a_first = __shfl_sync(kFull, a0, src);
+            const int before = __shfl_sync(kFull, drel - deg, src);  // entries before row jr
+            int len = 0;
+            int bs = 0;
+            V av = V(0);
+            if (f < dtotal) {
+                const int ai = a_first + (f - before);
+                const int k = __ldg(p.a_col + ai);
+                av = ldv<V>(p.a_val, ai);
+                bs = __ldg(p.b_rpt + k);
+                len = __ldg(p.b_rpt + k + 1) - bs;
+            }
+            const int lin = team_inclusive_scan<kWarp>(kFull, len, lane);
+            const int chunk = __shfl_sync(kFull, lin, 31);  // <= 32 - done
+            // lane t < chunk: product t's entry is the first lane with lin > t
+            int e = -1;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+                const int c = e + step;
+                const int v = __shfl_sync(kFull, lin, c & 31);
+                if (v <= lane) e = c;
+            }
+            e = (e + 1) & 31;
+            const int e_bs = __shfl_sync(kFull, bs, e);
+            const int e_first = __shfl_sync(kFull, lin - len, e);
+            const V e_av = __shfl_sync(kFull, av, e);
+            const int e_jr = __shfl_sync(kFull, jr, e);
+            const int e_row = __shfl_sync(kFull, row, e_jr & 31);
+            if (lane < chunk) {
+                const int qb = e_bs + (lane - e_first);
+                int32_t col = __ldg(p.b_col + qb);
+                const V prod = e_av * ldv<V>(p.b_val, qb);
+                // a column outside [0, B.n) would corrupt the packed key:
+                // report it, keep the key in range
+                if (static_cast<uint32_t>(col) >= static_cast<uint32_t>(p.n_cols)) {
+                    report(p.status, kStBadInput, e_row, col);
+                    col = 0;
+                }
+                const int pos = done + lane;
+                keys[pos] = (static_cast<uint32_t>(e_jr - j0) << 25) |
+                            (static_cast<uint32_t>(col) << 5) | static_cast<uint32_t>(pos);
+                vals[pos] = prod;
+            }
+            done += chunk;
+        }
+        __syncwarp();
+        const bool valid = lane < total;
+        uint32_t key = valid ? keys[lane] : 0xffffffffu;
+        // bitonic sort of the warp's 32 keys, ascending
+#pragma unroll
+        for (int k = 2; k <= kWarp; k <<= 1) {
+#pragma unroll
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                const uint32_t other = __shfl_xor_sync(kFull, key, j);
+                const bool asc = (lane & k) == 0;
+                const bool low = (lane & j) == 0;
+                key = (low == asc) ? min(key, other) : max(key, other);
+            }
+        }
+        sorted[lane] = key;
+        __syncwarp();
+        const uint32_t rc = key >> 5;  // (row in batch, column)
+        const uint32_t rr = key >> 25;
+        const uint32_t prev = __shfl_up_sync(kFull, key, 1);
+        const uint32_t next = __shfl_down_sync(kFull, key, 1);
+        const bool head = valid && (lane == 0 || (prev >> 5) != rc);
+        const bool rstart = valid && (lane == 0 || (prev >> 25) != rr);
+        const bool rend = valid && (lane == total - 1 || (next >> 25) != rr);
+        const unsigned heads = __ballot_sync(kFull, head);
+        const unsigned starts = __ballot_sync(kFull, rstart);
+        const unsigned upto = kFull >> (31 - lane);  // lanes <= this one
+        const int first = valid ? 31 - __clz(starts & upto) : 0;  // the row's first lane
+        const int rank = __popc(heads & upto & ~((1u << first) - 1u));  // heads of the row so far
+        const int jrow = (j0 + static_cast<int>(rr)) & 31;
+        const int out0 = __shfl_sync(kFull, c0, jrow);
+        const int out_row = __shfl_sync(kFull, row, jrow);
+        if (head) {
+            V sum = vals[key & 31u];
+            for (int k = lane + 1; k < total; k++) {
+                const uint32_t nk = sorted[k];
+                if ((nk >> 5) != rc) break;
+                sum += vals[nk & 31u];
+            }
+            p.c_col[out0 + rank - 1] = static_cast<int32_t>(rc & 0xfffffu);
+            static_cast<V*>(p.c_val)[out0 + rank - 1] = sum;
+        }
+        if (rend) p.row_nnz[out_row] = rank;
+        __syncwarp();
+        j0 = j1;
+    }
+}
+
 // Expand-sort-compress for rows of up to NMAX products with a whole CTA (the
 // 256-thread bin's range).  As the team version, with an unsigned key
 // (column << SHIFT | q), SHIFT = log2 of the sort capacity (B.n <= 2^(32 -
@@ -866,6 +1043,14 @@ cudaError_t launch_esc(const ProductArgs& p, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template<typename V>
+cudaError_t launch_esc_warp(const ProductArgs& p, cudaStream_t s) {
+    constexpr int R = kEscWarpThreads;  // 32 rows per warp
+    const int grid = (p.nrows + R - 1) / R;
+    k_esc_warp<V, kEscWarpThreads><<<grid, kEscWarpThreads, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
 template<typename V, int THREADS, int NMAX>
 cudaError_t launch_esc_cta(const ProductArgs& p, cudaStream_t s) {
     k_esc_cta<V, THREADS, NMAX><<<p.nrows, THREADS, EscCtaLayout<V, THREADS, NMAX>::bytes, s>>>(p);
@@ -1054,9 +1239,10 @@ B200_S2N_BITMAP_LADDER(double)
 B200_S2N_BITMAP_LADDER(float)
 #undef B200_S2N_BITMAP_LADDER
 
-// One-pass ladder for B.n <= kBitmapCols: the team bins and the 256-thread
-// bin expand, sort and compress (k_esc_team, k_esc_cta) with the hash bins'
-// row limits; the bitmap and global bins are the bitmap ladder's.
+// One-pass ladder for B.n <= kBitmapCols: the smallest rows packed many to a
+// warp (k_esc_warp), the team bins and the 256-thread bin expand, sort and
+// compress (k_esc_team, k_esc_cta) with the hash bins' row limits; the bitmap
+// and global bins are the bitmap ladder's.
 template<typename V>
 struct S2nEscLadder {
     static const BinLauncher entries[];
@@ -1066,8 +1252,8 @@ struct S2nEscLadder {
 #define B200_S2N_ESC_LADDER(V)                                                                \
     template<>                                                                                \
     const BinLauncher S2nEscLadder<V>::entries[] = {                                          \
-        {BinKind::Team, 12, 64, 256, EscLayout<V, 4, 256, 12>::bytes, "esc_team4_n12",        \
-         launch_esc<V, 4, 256, 12>},                                                          \
+        {BinKind::Team, 12, kEscWarpThreads, kEscWarpThreads, 0, "esc_warp_n12",              \
+         launch_esc_warp<V>},                                                                 \
         {BinKind::Team, 48, 32, 256, EscLayout<V, 8, 256, 48>::bytes, "esc_team8_n48",        \
          launch_esc<V, 8, 256, 48>},                                                          \
         {BinKind::Team, 192, 16, 256, EscLayout<V, 16, 256, 192>::bytes, "esc_team16_n192",   \
@@ -1114,7 +1300,6 @@ cudaError_t prepare_one() {
     B200_SMEM((k_s2n_cta<V, 1024, 43008, 32768>), (CtaLayout<1024, 43008, 32768>::bytes));
     B200_SMEM((k_s2n_bitmap<V, 1024, kBitmapCols>), (BitmapLayout<V, 1024, kBitmapCols>::bytes));
     B200_SMEM((k_s2n_bitmap_cluster<V, 1024>), (BitmapLayout<V, 1024, kBitmapCols>::bytes));
-    B200_SMEM((k_esc_team<V, 4, 256, 12>), (EscLayout<V, 4, 256, 12>::bytes));
     B200_SMEM((k_esc_team<V, 8, 256, 48>), (EscLayout<V, 8, 256, 48>::bytes));
     B200_SMEM((k_esc_team<V, 16, 256, 192>), (EscLayout<V, 16, 256, 192>::bytes));
     B200_SMEM((k_esc_team<V, 32, 256, 768>), (EscLayout<V, 32, 256, 768>::bytes));
