@@ -233,42 +233,56 @@ __global__ __launch_bounds__(THREADS) void k_esc_team(ProductArgs p) {
     if (lane == 0) p.row_nnz[row] = written;
 }
 
-// Expand-sort-compress of the smallest rows (the first one-pass bin) with
-// whole warps over many rows.  A team of G lanes per row leaves most lanes
-// idle there: the 1M power-law product has 826 k rows of 1-12 products, 2.9 on
-// average (ncu: 9 of 32 lanes active per instruction with 4-lane teams).  A
-// warp takes 32 rows of the bin's list and packs them, in list order, into
-// batches of at most 32 products, one per lane.  Per batch:
+// Expand-sort-compress of the small rows (the first three one-pass bins, up
+// to 192 products) with whole warps over many rows.  A team of G lanes per row
+// leaves most lanes idle there: the 1M power-law product has 826 k rows of
+// 1-12 products, 2.9 on average (ncu: 9 of 32 lanes active per instruction
+// with 4-lane teams).  A warp takes ROWS rows of the bin's list and packs
+// them, in list order, into batches of at most 32 K products, K per lane.
+// Per batch:
 //   1. the batch's A entries, flattened over its rows, 32 at a time: each lane
 //      finds its entry's row by a search over the rows' A-entry prefix (held
 //      one per lane), loads the entry and its B row's extent, and a warp scan
 //      of the B-row lengths places each entry's first product;
-//   2. each lane finds its product's entry by a search over that scan, loads
-//      B's column and value, and stages the key (row in the batch << 25 |
-//      column << 5 | product) and the product a_ik * b_kj in shared memory;
-//   3. a warp bitonic sort of the 32 keys orders them by row, column and
-//      product; the first lane of each (row, column) run sums the run in
-//      product order (Gustavson's order, as the team kernels) and writes the
-//      column and sum at its rank in the row; the last lane of each row
-//      writes the row's nnz.
+//   2. 32 products at a time, each lane finds its product's entry by a search
+//      over that scan, loads B's column and value, and stages the key (row in
+//      the batch << (20 + PB) | column << PB | product, PB = log2(32 K); the
+//      three fit 32 bits) and the product a_ik * b_kj in shared memory;
+//   3. a warp bitonic sort of the 32 K keys (element r * 32 + lane in
+//      register r of the lane) orders them by row, column and product; the
+//      first element of each (row, column) run sums the run in product order
+//      (Gustavson's order, as the team kernels) and writes the column and sum
+//      at its rank in the row; the last element of each row writes the row's
+//      nnz.
 // Single-entry rows take the same path.  Needs B.n <= 2^20 (the ladder that
-// holds it) and the one-pass mode's NIP-sized slots; a row of more than 32
-// products is reported.
+// holds it) and the one-pass mode's NIP-sized slots; a row of more than 32 K
+// products is reported.  Per bin (1M power-law product, serialised): rows of
+// <= 12 products K = 1, 32 rows a warp (4-lane teams 0.092 -> 0.057 ms); <= 48
+// K = 2, 8 rows (8-lane teams 0.067 -> 0.060; 4 or 16 rows no better); <= 192
+// K = 8, 4 rows (16-lane teams 0.117 -> 0.104; 2 rows 0.103 but the product
+// 1.108 -> 1.112 ms).
 constexpr int kEscWarpThreads = 256;
 
-template<typename V, int THREADS>
+
+template<typename V, int THREADS, int K, int ROWS>
 __global__ __launch_bounds__(THREADS) void k_esc_warp(ProductArgs p) {
+    static_assert(K == 1 || K == 2 || K == 4 || K == 8, "keys per lane");
+    static_assert(ROWS >= 1 && ROWS <= kWarp, "rows per warp");
     constexpr int NW = THREADS / kWarp;
+    constexpr int CAP = kWarp * K;  // products per batch
+    constexpr int PB = ilog2(CAP);  // bits of a product's place in the batch
+    constexpr int RS = 20 + PB;     // row-in-batch shift
+    static_assert(RS + ilog2(2 * ROWS - 1) <= 32, "row, column and place fit 32 bits");
     constexpr unsigned kFull = 0xffffffffu;
-    __shared__ uint32_t s_key[NW][kWarp];
-    __shared__ uint32_t s_sorted[NW][kWarp];
-    __shared__ V s_val[NW][kWarp];
+    __shared__ uint32_t s_key[NW][CAP];
+    __shared__ uint32_t s_sorted[NW][CAP];
+    __shared__ V s_val[NW][CAP];
     const int lane = static_cast<int>(threadIdx.x & 31u);
     const int w = static_cast<int>(threadIdx.x >> 5);
-    const int r0 = (blockIdx.x * NW + w) * kWarp;
+    const int r0 = (blockIdx.x * NW + w) * ROWS;
     if (r0 >= p.nrows) return;  // uniform over the warp
-    const int nr = min(kWarp, p.nrows - r0);
-    // lane j holds row j of the warp's rows
+    const int nr = min(ROWS, p.nrows - r0);
+    // lane j < nr holds row j of the warp's rows
     int row = 0;
     int c0 = 0;
     int nip = 0;
@@ -280,7 +294,7 @@ __global__ __launch_bounds__(THREADS) void k_esc_warp(ProductArgs p) {
         nip = p.c_rpt[row + 1] - c0;  // the row's NIP-sized slot
         a0 = p.a_rpt[row];
         deg = p.a_rpt[row + 1] - a0;
-        if (nip > kWarp || nip < 0 || p.row_nnz == nullptr) {
+        if (nip > CAP || nip < 0 || p.row_nnz == nullptr) {
             report(p.status, kStCapacity, row, nip);
             nip = 0;  // left out; the status fails the product
             deg = 0;
@@ -297,9 +311,9 @@ __global__ __launch_bounds__(THREADS) void k_esc_warp(ProductArgs p) {
     for (int j0 = 0; j0 < nr;) {  // uniform over the warp
         const int pbase = j0 > 0 ? __shfl_sync(kFull, pin, j0 - 1) : 0;
         const int dbase = j0 > 0 ? __shfl_sync(kFull, din, j0 - 1) : 0;
-        // rows [j0, j1): the longest run from j0 whose products fit 32 (row j0
-        // always does; pin is non-decreasing, so the run is contiguous)
-        const unsigned take = __ballot_sync(kFull, lane >= j0 && lane < nr && pin - pbase <= kWarp);
+        // rows [j0, j1): the longest run from j0 whose products fit CAP (row
+        // j0 always does; pin is non-decreasing, so the run is contiguous)
+        const unsigned take = __ballot_sync(kFull, lane >= j0 && lane < nr && pin - pbase <= CAP);
         const int j1 = 32 - __clz(take);
         const int total = __shfl_sync(kFull, pin, j1 - 1) - pbase;
         const int dtotal = __shfl_sync(kFull, din, j1 - 1) - dbase;
@@ -331,80 +345,141 @@ __global__ __launch_bounds__(THREADS) void k_esc_warp(ProductArgs p) {
                 len = __ldg(p.b_rpt + k + 1) - bs;
             }
             const int lin = team_inclusive_scan<kWarp>(kFull, len, lane);
-            const int chunk = __shfl_sync(kFull, lin, 31);  // <= 32 - done
-            // lane t < chunk: product t's entry is the first lane with lin > t
-            int e = -1;
+            const int chunk = __shfl_sync(kFull, lin, 31);  // <= CAP - done
 #pragma unroll
-            for (int step = 16; step >= 1; step >>= 1) {
-                const int c = e + step;
-                const int v = __shfl_sync(kFull, lin, c & 31);
-                if (v <= lane) e = c;
-            }
-            e = (e + 1) & 31;
-            const int e_bs = __shfl_sync(kFull, bs, e);
-            const int e_first = __shfl_sync(kFull, lin - len, e);
-            const V e_av = __shfl_sync(kFull, av, e);
-            const int e_jr = __shfl_sync(kFull, jr, e);
-            const int e_row = __shfl_sync(kFull, row, e_jr & 31);
-            if (lane < chunk) {
-                const int qb = e_bs + (lane - e_first);
-                int32_t col = __ldg(p.b_col + qb);
-                const V prod = e_av * ldv<V>(p.b_val, qb);
-                // a column outside [0, B.n) would corrupt the packed key:
-                // report it, keep the key in range
-                if (static_cast<uint32_t>(col) >= static_cast<uint32_t>(p.n_cols)) {
-                    report(p.status, kStBadInput, e_row, col);
-                    col = 0;
+            for (int t0 = 0; t0 < CAP; t0 += kWarp) {
+                if (t0 >= chunk) break;  // uniform over the warp
+                const int t = t0 + lane;
+                // product t's entry: the first lane with lin > t
+                int e = -1;
+#pragma unroll
+                for (int step = 16; step >= 1; step >>= 1) {
+                    const int c = e + step;
+                    const int v = __shfl_sync(kFull, lin, c & 31);
+                    if (v <= t) e = c;
                 }
-                const int pos = done + lane;
-                keys[pos] = (static_cast<uint32_t>(e_jr - j0) << 25) |
-                            (static_cast<uint32_t>(col) << 5) | static_cast<uint32_t>(pos);
-                vals[pos] = prod;
+                e = (e + 1) & 31;
+                const int e_bs = __shfl_sync(kFull, bs, e);
+                const int e_first = __shfl_sync(kFull, lin - len, e);
+                const V e_av = __shfl_sync(kFull, av, e);
+                const int e_jr = __shfl_sync(kFull, jr, e);
+                const int e_row = __shfl_sync(kFull, row, e_jr & 31);
+                if (t < chunk) {
+                    const int qb = e_bs + (t - e_first);
+                    int32_t col = __ldg(p.b_col + qb);
+                    const V prod = e_av * ldv<V>(p.b_val, qb);
+                    // a column outside [0, B.n) would corrupt the packed key:
+                    // report it, keep the key in range
+                    if (static_cast<uint32_t>(col) >= static_cast<uint32_t>(p.n_cols)) {
+                        report(p.status, kStBadInput, e_row, col);
+                        col = 0;
+                    }
+                    const int pos = done + t;
+                    keys[pos] = (static_cast<uint32_t>(e_jr - j0) << RS) |
+                                (static_cast<uint32_t>(col) << PB) | static_cast<uint32_t>(pos);
+                    vals[pos] = prod;
+                }
             }
             done += chunk;
         }
         __syncwarp();
-        const bool valid = lane < total;
-        uint32_t key = valid ? keys[lane] : 0xffffffffu;
-        // bitonic sort of the warp's 32 keys, ascending
+        uint32_t key[K];
 #pragma unroll
-        for (int k = 2; k <= kWarp; k <<= 1) {
+        for (int r = 0; r < K; r++) {
+            const int i = r * kWarp + lane;
+            key[r] = i < total ? keys[i] : 0xffffffffu;
+        }
+        // bitonic sort of the warp's CAP keys, ascending; element i = r * 32 + lane
+#pragma unroll
+        for (int k = 2; k <= CAP; k <<= 1) {
 #pragma unroll
             for (int j = k >> 1; j > 0; j >>= 1) {
-                const uint32_t other = __shfl_xor_sync(kFull, key, j);
-                const bool asc = (lane & k) == 0;
-                const bool low = (lane & j) == 0;
-                key = (low == asc) ? min(key, other) : max(key, other);
+                if (j >= kWarp) {  // partner in another register of this lane
+                    const int jr = j / kWarp;
+#pragma unroll
+                    for (int r = 0; r < K; r++) {
+                        if ((r & jr) == 0) {
+                            const bool asc = ((r * kWarp + lane) & k) == 0;
+                            const uint32_t x = key[r];
+                            const uint32_t y = key[r + jr];
+                            key[r] = asc ? min(x, y) : max(x, y);
+                            key[r + jr] = asc ? max(x, y) : min(x, y);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < K; r++) {
+                        const uint32_t other = __shfl_xor_sync(kFull, key[r], j);
+                        const bool asc = ((r * kWarp + lane) & k) == 0;
+                        const bool low = (lane & j) == 0;
+                        key[r] = (low == asc) ? min(key[r], other) : max(key[r], other);
+                    }
+                }
             }
         }
-        sorted[lane] = key;
+#pragma unroll
+        for (int r = 0; r < K; r++) sorted[r * kWarp + lane] = key[r];
         __syncwarp();
-        const uint32_t rc = key >> 5;  // (row in batch, column)
-        const uint32_t rr = key >> 25;
-        const uint32_t prev = __shfl_up_sync(kFull, key, 1);
-        const uint32_t next = __shfl_down_sync(kFull, key, 1);
-        const bool head = valid && (lane == 0 || (prev >> 5) != rc);
-        const bool rstart = valid && (lane == 0 || (prev >> 25) != rr);
-        const bool rend = valid && (lane == total - 1 || (next >> 25) != rr);
-        const unsigned heads = __ballot_sync(kFull, head);
-        const unsigned starts = __ballot_sync(kFull, rstart);
-        const unsigned upto = kFull >> (31 - lane);  // lanes <= this one
-        const int first = valid ? 31 - __clz(starts & upto) : 0;  // the row's first lane
-        const int rank = __popc(heads & upto & ~((1u << first) - 1u));  // heads of the row so far
-        const int jrow = (j0 + static_cast<int>(rr)) & 31;
-        const int out0 = __shfl_sync(kFull, c0, jrow);
-        const int out_row = __shfl_sync(kFull, row, jrow);
-        if (head) {
-            V sum = vals[key & 31u];
-            for (int k = lane + 1; k < total; k++) {
-                const uint32_t nk = sorted[k];
-                if ((nk >> 5) != rc) break;
-                sum += vals[nk & 31u];
-            }
-            p.c_col[out0 + rank - 1] = static_cast<int32_t>(rc & 0xfffffu);
-            static_cast<V*>(p.c_val)[out0 + rank - 1] = sum;
+        // per register: run heads and row starts
+        unsigned heads[K];
+        unsigned starts[K];
+#pragma unroll
+        for (int r = 0; r < K; r++) {
+            const int i = r * kWarp + lane;
+            const bool valid = i < total;
+            // element i - 1: this register of the lane below, or the last
+            // lane's previous register
+            const uint32_t up = __shfl_up_sync(kFull, key[r], 1);
+            const uint32_t carry = __shfl_sync(kFull, key[r > 0 ? r - 1 : 0], 31);
+            const uint32_t prev = lane > 0 ? up : (r > 0 ? carry : 0xffffffffu);
+            heads[r] = __ballot_sync(kFull, valid && (i == 0 || (prev >> PB) != (key[r] >> PB)));
+            starts[r] = __ballot_sync(kFull, valid && (i == 0 || (prev >> RS) != (key[r] >> RS)));
         }
-        if (rend) p.row_nnz[out_row] = rank;
+        const unsigned upto = kFull >> (31 - lane);  // lanes <= this one
+#pragma unroll
+        for (int r = 0; r < K; r++) {
+            const int i = r * kWarp + lane;
+            const bool valid = i < total;
+            const uint32_t kr = key[r];
+            const uint32_t rr = kr >> RS;
+            // the row's first element f: the last row start at or before i
+            int f = 0;
+#pragma unroll
+            for (int q = 0; q <= r; q++) {
+                const unsigned m = q < r ? starts[q] : (starts[q] & upto);
+                if (m != 0u) f = q * kWarp + 31 - __clz(m);
+            }
+            // heads in [f, i]
+            int rank = 0;
+#pragma unroll
+            for (int q = 0; q <= r; q++) {
+                unsigned m = q < r ? heads[q] : (heads[q] & upto);
+                const int fq = f - q * kWarp;  // f's lane in register q, if there
+                if (fq >= kWarp) m = 0u;
+                else if (fq > 0) m &= ~((1u << fq) - 1u);
+                rank += __popc(m);
+            }
+            const int jrow = (j0 + static_cast<int>(rr)) & 31;
+            const int out0 = __shfl_sync(kFull, c0, jrow);
+            const int out_row = __shfl_sync(kFull, row, jrow);
+            const bool head = valid && ((heads[r] >> lane) & 1u);
+            if (head) {
+                V sum = vals[kr & (CAP - 1)];
+                for (int x = i + 1; x < total; x++) {
+                    const uint32_t nk = sorted[x];
+                    if ((nk >> PB) != (kr >> PB)) break;
+                    sum += vals[nk & (CAP - 1)];
+                }
+                p.c_col[out0 + rank - 1] = static_cast<int32_t>((kr >> PB) & 0xfffffu);
+                static_cast<V*>(p.c_val)[out0 + rank - 1] = sum;
+            }
+            const uint32_t down = __shfl_down_sync(kFull, kr, 1);
+            const uint32_t wrap = __shfl_sync(kFull, key[r + 1 < K ? r + 1 : r], 0);
+            const uint32_t next =
+                i + 1 >= total ? 0xffffffffu : lane < 31 ? down : (r + 1 < K ? wrap : 0xffffffffu);
+            const bool rend = valid && (i == total - 1 || (next >> RS) != rr);
+            if (rend) p.row_nnz[out_row] = rank;
+        }
         __syncwarp();
         j0 = j1;
     }
@@ -1043,11 +1118,11 @@ cudaError_t launch_esc(const ProductArgs& p, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-template<typename V>
+template<typename V, int K, int ROWS>
 cudaError_t launch_esc_warp(const ProductArgs& p, cudaStream_t s) {
-    constexpr int R = kEscWarpThreads;  // 32 rows per warp
+    constexpr int R = kEscWarpThreads / kWarp * ROWS;  // rows per CTA
     const int grid = (p.nrows + R - 1) / R;
-    k_esc_warp<V, kEscWarpThreads><<<grid, kEscWarpThreads, 0, s>>>(p);
+    k_esc_warp<V, kEscWarpThreads, K, ROWS><<<grid, kEscWarpThreads, 0, s>>>(p);
     return cudaGetLastError();
 }
 
@@ -1253,11 +1328,11 @@ struct S2nEscLadder {
     template<>                                                                                \
     const BinLauncher S2nEscLadder<V>::entries[] = {                                          \
         {BinKind::Team, 12, kEscWarpThreads, kEscWarpThreads, 0, "esc_warp_n12",              \
-         launch_esc_warp<V>},                                                                 \
-        {BinKind::Team, 48, 32, 256, EscLayout<V, 8, 256, 48>::bytes, "esc_team8_n48",        \
-         launch_esc<V, 8, 256, 48>},                                                          \
-        {BinKind::Team, 192, 16, 256, EscLayout<V, 16, 256, 192>::bytes, "esc_team16_n192",   \
-         launch_esc<V, 16, 256, 192>},                                                        \
+         launch_esc_warp<V, 1, 32>},                                                          \
+        {BinKind::Team, 48, kEscWarpThreads / kWarp * 8, kEscWarpThreads, 0, "esc_warp2_n48",  \
+         launch_esc_warp<V, 2, 8>},                                                           \
+        {BinKind::Team, 192, kEscWarpThreads / kWarp * 4, kEscWarpThreads, 0,                  \
+         "esc_warp8_n192", launch_esc_warp<V, 8, 4>},                                         \
         {BinKind::Team, 768, 8, 256, EscLayout<V, 32, 256, 768>::bytes, "esc_team32_n768",    \
          launch_esc<V, 32, 256, 768>},                                                        \
         {BinKind::Cta, 3072, 1, 256, EscCtaLayout<V, 256, 3072>::bytes, "esc_cta256_n3072",    \
@@ -1300,8 +1375,6 @@ cudaError_t prepare_one() {
     B200_SMEM((k_s2n_cta<V, 1024, 43008, 32768>), (CtaLayout<1024, 43008, 32768>::bytes));
     B200_SMEM((k_s2n_bitmap<V, 1024, kBitmapCols>), (BitmapLayout<V, 1024, kBitmapCols>::bytes));
     B200_SMEM((k_s2n_bitmap_cluster<V, 1024>), (BitmapLayout<V, 1024, kBitmapCols>::bytes));
-    B200_SMEM((k_esc_team<V, 8, 256, 48>), (EscLayout<V, 8, 256, 48>::bytes));
-    B200_SMEM((k_esc_team<V, 16, 256, 192>), (EscLayout<V, 16, 256, 192>::bytes));
     B200_SMEM((k_esc_team<V, 32, 256, 768>), (EscLayout<V, 32, 256, 768>::bytes));
     B200_SMEM((k_esc_team<V, 32, 256, kEscSplit>), (EscLayout<V, 32, 256, kEscSplit>::bytes));
     B200_SMEM((k_esc_cta<V, 256, 3072>), (EscCtaLayout<V, 256, 3072>::bytes));
