@@ -55,8 +55,8 @@ def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None,
-                    help="timed steps (default: 50 for the plain product, whose step "
-                         "takes ~1.4 ms, so that clocks are sampled inside the region; "
+                    help="timed steps (default: 100 for the plain product, whose step "
+                         "takes ~1.1 ms, so that clocks are sampled inside the region; "
                          "10 for the other modes)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
@@ -166,8 +166,11 @@ def replica_gflops(nip: int, steps: int, world: int, max_ms: float) -> float:
 
 class ClockSampler:
     """SM clock and clock-event reasons sampled DURING a timed region: NVML
-    polled every 5 ms from a thread (a timed region of a few steps lasts only
-    milliseconds); nvidia-smi at its 200 ms minimum if NVML is unavailable.
+    polled every 25 ms from a thread; nvidia-smi at its 200 ms minimum if NVML
+    is unavailable.  Polling every 5 ms stalled about one product in 50 by
+    ~1 ms on a B200 (each poll's driver calls contend with the product's own
+    synchronisations), which moved the plain product's mean by 2 %; at 25 ms
+    the timed region of 100 products still sees several samples.
     Reads only -- no setting of the GPU is touched."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -205,7 +208,7 @@ class ClockSampler:
                 self.samples.append((float(sm), float(mx), int(rs)))
             except Exception:
                 pass
-            self.stop.wait(0.005)
+            self.stop.wait(0.025)
 
     def __enter__(self):
         try:
@@ -256,7 +259,7 @@ class ClockSampler:
                 for nm, const in self.REASONS.items():
                     if bits & int(getattr(self.nvml, const, 0)):
                         reasons.add(nm)
-            source = "nvml, 5 ms"
+            source = "nvml, 25 ms"
         else:
             names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
             for ln in self.lines:
@@ -525,6 +528,8 @@ def run_ours(args, rank, world, local_rank):
     line = {
         "metric": metric_name(args.dtype), "value": value, "unit": "GFLOPS", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "step_ms": {"min": float(np.min(step_ms)), "median": float(np.median(step_ms)),
+                    "max": float(np.max(step_ms)), "first": float(step_ms[0])},
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": args.dtype, "data": "synthetic (seeded generator)",
         "config": config_of(args, A, nip, nnz_c),
@@ -727,6 +732,7 @@ def run_galerkin(args, local_rank):
                          f"{(A_h.nnz * (4 + A_h.val.itemsize)) >> 20} MB)"},
         "stages_ms": {"transpose_P": float(np.mean(t_tr)), "A_times_P": float(np.mean(t_ap)),
                       "R_times_AP": float(np.mean(t_rap))},
+        "call_ms_per_step": [round(float(t), 4) for t in t_call],
         "e2e": {"value": flops / (e2e_ms / 1e3) / 1e9, "unit": "GFLOPS",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": e2e_ms},
@@ -899,7 +905,7 @@ def run_served(args, local_rank):
 def main():
     args = parse()
     if args.steps is None:
-        args.steps = 50 if args.mode == "plain" and args.impl == "ours" else 10
+        args.steps = 100 if args.mode == "plain" and args.impl == "ours" else 10
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -34,21 +34,29 @@ __device__ __forceinline__ long long warp_sum_ll(long long v) {
 }
 
 // ---- pass 1: NIP per row (setup.cuh:29-95) + histogram --------------------
-__global__ __launch_bounds__(kBinThreads) void k_nip_hist(
+constexpr int kNipThreads = 256;  // kBinRowsPerCta rows per CTA, as the other passes
+
+__global__ __launch_bounds__(kNipThreads) void k_nip_hist(
     const int32_t* __restrict__ a_rpt, const int32_t* __restrict__ a_col,
     const int32_t* __restrict__ b_rpt, int32_t m, int32_t* __restrict__ c_rpt,
     int32_t* __restrict__ nip_copy, int32_t* __restrict__ hist, Plan* __restrict__ plan,
-    DevStatus* __restrict__ st, const __grid_constant__ Ladder lad) {
+    DevStatus* __restrict__ st, const __grid_constant__ Ladder lad,
+    int32_t* __restrict__ hist_fill, int64_t* __restrict__ cta_sum,
+    const __grid_constant__ Ladder fill) {
     __shared__ int32_t s_hist[kMaxBins];
-    __shared__ long long s_tot[kBinThreads / kWarp];
-    __shared__ int32_t s_max[kBinThreads / kWarp];
+    __shared__ int32_t s_hist_fill[kMaxBins];
+    __shared__ long long s_tot[kNipThreads / kWarp];
+    __shared__ int32_t s_max[kNipThreads / kWarp];
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int w = tid >> 5;
-    if (tid < kMaxBins) s_hist[tid] = 0;
+    if (tid < kMaxBins) {
+        s_hist[tid] = 0;
+        s_hist_fill[tid] = 0;
+    }
     __syncthreads();
 
-    constexpr int kGroups = kBinRowsPerCta / kWarp / (kBinThreads / kWarp);  // per warp
+    constexpr int kGroups = kBinRowsPerCta / kWarp / (kNipThreads / kWarp);  // per warp
     long long my_tot = 0;
     int32_t my_max = 0;
     for (int j = 0; j < kGroups; j++) {
@@ -106,7 +114,10 @@ __global__ __launch_bounds__(kBinThreads) void k_nip_hist(
             if (nip_copy != nullptr) nip_copy[r] = key;
             my_tot += nip;
             my_max = max(my_max, key);
-            if (key > 0) atomicAdd(&s_hist[find_bin(lad, key)], 1);
+            if (key > 0) {
+                atomicAdd(&s_hist[find_bin(lad, key)], 1);
+                if (hist_fill != nullptr) atomicAdd(&s_hist_fill[find_bin(fill, key)], 1);
+            }
         }
     }
     my_tot = warp_sum_ll(my_tot);
@@ -119,15 +130,19 @@ __global__ __launch_bounds__(kBinThreads) void k_nip_hist(
     if (tid == 0) {
         long long t = 0;
         int32_t mx = 0;
-        for (int i = 0; i < kBinThreads / kWarp; i++) {
+        for (int i = 0; i < kNipThreads / kWarp; i++) {
             t += s_tot[i];
             mx = max(mx, s_max[i]);
         }
         atomicAdd(reinterpret_cast<unsigned long long*>(&plan->total_key),
                   static_cast<unsigned long long>(t));
         atomicMax(&plan->max_key, mx);
+        if (cta_sum != nullptr) cta_sum[blockIdx.x] = t;
     }
-    if (tid < kMaxBins) hist[blockIdx.x * kMaxBins + tid] = s_hist[tid];
+    if (tid < kMaxBins) {
+        hist[blockIdx.x * kMaxBins + tid] = s_hist[tid];
+        if (hist_fill != nullptr) hist_fill[blockIdx.x * kMaxBins + tid] = s_hist_fill[tid];
+    }
 }
 
 // ---- pass 1': nnz histogram + per-CTA nnz sums ----------------------------
@@ -234,12 +249,141 @@ __global__ __launch_bounds__(kOffThreads) void k_bin_offsets(int32_t* __restrict
     }
 }
 
+// ---- pass 2, all bins at once (one CTA) ------------------------------------
+// The per-CTA histograms src_hist[i][e] count rows by a source ladder `src`
+// (e.g. the NIP pass's fill ladder, whose limits include every limit the
+// device may choose); each source bin maps to the final ladder's bin (dlad
+// when given, else lad) that holds its upper limit.  hist[i][b] receives CTA
+// i's first position in final bin b RELATIVE to the bin's start (the scatter
+// adds plan->bin_off), cta_sum (when given) its exclusive scan.  Per chunk of
+// kOffMapChunk CTAs: every thread stages one CTA's final-bin counts in shared
+// memory, then a warp per bin (and one for the CTA sums) scans them -- each
+// lane 32 consecutive CTAs, one warp scan of the lanes' sums.  One pass over
+// the histograms and two block barriers per chunk, where k_bin_offsets scans
+// bin after bin with the whole CTA.
+constexpr int kOffMapThreads = 1024;
+constexpr int kOffMapChunk = kOffMapThreads;  // a CTA's count in a bin fits 16 bits
+
+// staged element j of a chunk: one spare slot per 32 keeps the lanes' runs of
+// 32 in distinct banks
+__device__ __forceinline__ int offmap_pad(int j) { return j + (j >> 5); }
+
+__global__ __launch_bounds__(kOffMapThreads) void k_bin_offsets_map(
+    const int32_t* __restrict__ src_hist, int32_t* __restrict__ hist, int32_t nctas,
+    const __grid_constant__ Ladder src, int64_t* __restrict__ cta_sum, Plan* __restrict__ plan,
+    const __grid_constant__ Ladder lad, const Ladder* __restrict__ dlad) {
+    constexpr int NW = kOffMapThreads / kWarp;
+    constexpr int PADDED = kOffMapChunk + kOffMapChunk / kWarp;
+    static_assert(NW > kMaxBins, "a warp per bin and one for the CTA sums");
+    static_assert(kBinRowsPerCta < 65536, "16-bit counts");
+    __shared__ uint16_t s_cnt[kMaxBins][PADDED + 1];
+    __shared__ long long s_sum[PADDED];
+    __shared__ int32_t s_map[kMaxBins];
+    __shared__ int32_t s_e0[kMaxBins];
+    __shared__ int32_t s_e1[kMaxBins];
+    __shared__ int32_t s_tot[kMaxBins];
+    const Ladder& L = dlad != nullptr ? *dlad : lad;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int w = tid >> 5;
+    const int nb = L.nb;
+    const int ne = src.nb;
+    const bool sums = cta_sum != nullptr;
+    if (tid < kMaxBins) {
+        int b = nb - 1;
+        if (tid < ne) {
+            const int32_t u = src.limit[tid];
+            for (int i = 0; i < nb; i++) {
+                if (u <= L.limit[i]) {
+                    b = i;
+                    break;
+                }
+            }
+            b = b < L.min_bin ? L.min_bin : b;
+        }
+        s_map[tid] = b;
+        s_e0[tid] = ne;
+        s_e1[tid] = ne;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        // each final bin's range of source bins (the map is monotone; empty
+        // ranges start at ne)
+        for (int e = ne - 1; e >= 0; e--) s_e0[s_map[e]] = e;
+        for (int e = 0; e < ne; e++) s_e1[s_map[e]] = e + 1;
+        for (int b = 0; b < nb; b++)
+            if (s_e1[b] < s_e0[b]) s_e1[b] = s_e0[b];
+    }
+    __syncthreads();
+    const bool scans_bin = w < nb;
+    const bool scans_sums = w == NW - 1 && sums;
+    long long run = 0;  // this warp's bin (or the CTA sums) so far
+    for (int c0 = 0; c0 < nctas; c0 += kOffMapChunk) {
+        // stage: thread tid holds CTA c0 + tid
+        {
+            const int i = c0 + tid;
+            for (int b = 0; b < nb; b++) {
+                int32_t c = 0;
+                if (i < nctas)
+                    for (int e = s_e0[b]; e < s_e1[b]; e++) c += src_hist[i * kMaxBins + e];
+                s_cnt[b][offmap_pad(tid)] = static_cast<uint16_t>(c);
+            }
+            if (sums) s_sum[offmap_pad(tid)] = i < nctas ? cta_sum[i] : 0;
+        }
+        __syncthreads();
+        if (scans_bin || scans_sums) {
+            // lane: CTAs [c0 + 32 lane, c0 + 32 lane + 32)
+            long long part = 0;
+#pragma unroll 8
+            for (int k = 0; k < kWarp; k++) {
+                const int j = offmap_pad(lane * kWarp + k);
+                part += scans_bin ? static_cast<long long>(s_cnt[w][j]) : s_sum[j];
+            }
+            long long x = part;
+#pragma unroll
+            for (int o = 1; o < kWarp; o <<= 1) {
+                const long long t = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += t;
+            }
+            long long acc = run + x - part;
+            for (int k = 0; k < kWarp; k++) {
+                const int i = c0 + lane * kWarp + k;
+                if (i >= nctas) break;
+                const int j = offmap_pad(lane * kWarp + k);
+                if (scans_bin) {
+                    hist[i * kMaxBins + w] = static_cast<int32_t>(acc);
+                    acc += s_cnt[w][j];
+                } else {
+                    cta_sum[i] = acc;
+                    acc += s_sum[j];
+                }
+            }
+            run += __shfl_sync(0xffffffffu, x, kWarp - 1);
+        }
+        __syncthreads();
+    }
+    if (scans_bin && lane == 0) s_tot[w] = static_cast<int32_t>(run);
+    if (scans_sums && lane == 0) {
+        plan->total_key = run;
+        plan->overflow = run > INT32_MAX ? 1 : 0;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int32_t off = 0;
+        for (int b = 0; b < nb; b++) {
+            plan->bin_size[b] = s_tot[b];
+            plan->bin_off[b] = off;
+            off += s_tot[b];
+        }
+    }
+}
+
 // ---- pass 3: stable scatter (+ exclusive scan into C.rpt) ------------------
 __global__ __launch_bounds__(kBinThreads) void k_bin_scatter(
     int32_t* __restrict__ c_rpt, int32_t m, const int32_t* __restrict__ hist_off,
     const int64_t* __restrict__ cta_off, int32_t* __restrict__ bins,
     const Plan* __restrict__ plan, const __grid_constant__ Ladder lad, int scan,
-    const Ladder* __restrict__ dlad) {
+    const Ladder* __restrict__ dlad, int bin_relative) {
     const Ladder& L = dlad != nullptr ? *dlad : lad;  // limits chosen on the device, if any
     constexpr int NW = kBinThreads / kWarp;
     __shared__ int32_t s_base[kMaxBins];
@@ -252,7 +396,9 @@ __global__ __launch_bounds__(kBinThreads) void k_bin_scatter(
     const int w = tid >> 5;
     if (tid < kMaxBins) {
         s_base[tid] = 0;
-        s_off[tid] = hist_off[blockIdx.x * kMaxBins + tid];
+        // offsets within each bin (k_bin_offsets_map) or of the row list
+        s_off[tid] = hist_off[blockIdx.x * kMaxBins + tid] +
+                     (bin_relative && tid < L.nb ? plan->bin_off[tid] : 0);
     }
     if (tid == 0) s_run = 0;
     const long long base_rpt = scan ? cta_off[blockIdx.x] : 0;
@@ -302,6 +448,115 @@ __global__ __launch_bounds__(kBinThreads) void k_bin_scatter(
     }
     if (scan && blockIdx.x == gridDim.x - 1 && tid == 0) {
         c_rpt[m] = static_cast<int32_t>(plan->total_key);
+    }
+}
+
+// ---- one-pass row pointer: reduce, then scan --------------------------------
+// The rows' nnz become the row pointer in two launches: k_rpt_reduce sums (and
+// maxes) each tile of kScanTile counts; k_rpt_scan adds the sums of the tiles
+// before its own (read by each CTA itself) to an in-place exclusive scan of
+// its tile.  12 bytes of traffic per row, where a one-bin pass of the binning
+// kernels takes three launches and also writes a row list.
+constexpr int kScanThreads = 256;
+constexpr int kScanPer = kScanTile / kScanThreads;  // rows per thread
+static_assert(kScanPer * kScanThreads == kScanTile, "tile");
+
+__global__ __launch_bounds__(kScanThreads) void k_rpt_reduce(const int32_t* __restrict__ cnt,
+                                                             int32_t m,
+                                                             int64_t* __restrict__ tile_sum,
+                                                             Plan* __restrict__ plan) {
+    __shared__ long long s_sum[kScanThreads / kWarp];
+    __shared__ int32_t s_max[kScanThreads / kWarp];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int w = tid >> 5;
+    const long long r0 = static_cast<long long>(blockIdx.x) * kScanTile;
+    long long sum = 0;
+    int32_t mx = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) {
+        const long long r = r0 + k * kScanThreads + tid;
+        if (r < m) {
+            const int32_t v = cnt[r];
+            sum += v;
+            mx = max(mx, v);
+        }
+    }
+    sum = warp_sum_ll(sum);
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if (lane == 0) {
+        s_sum[w] = sum;
+        s_max[w] = mx;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        long long t = 0;
+        int32_t x = 0;
+        for (int i = 0; i < kScanThreads / kWarp; i++) {
+            t += s_sum[i];
+            x = max(x, s_max[i]);
+        }
+        tile_sum[blockIdx.x] = t;
+        atomicMax(&plan->max_key, x);
+    }
+}
+
+// the tile in shared memory, one padding word per 32 (thread t reads its
+// kScanPer consecutive rows without bank conflicts)
+__device__ __forceinline__ int scan_pad(int i) { return i + (i >> 5); }
+
+__global__ __launch_bounds__(kScanThreads) void k_rpt_scan(int32_t* __restrict__ cnt, int32_t m,
+                                                           const int64_t* __restrict__ tile_sum,
+                                                           Plan* __restrict__ plan) {
+    __shared__ int32_t s_row[kScanTile + kScanTile / 32];
+    __shared__ long long s_before[kScanThreads / kWarp];
+    __shared__ int32_t s_wtot[kScanThreads / kWarp];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int w = tid >> 5;
+    // the counts of the tiles before this one
+    long long before = 0;
+    for (int t = tid; t < static_cast<int>(blockIdx.x); t += kScanThreads) before += tile_sum[t];
+    before = warp_sum_ll(before);
+    if (lane == 0) s_before[w] = before;
+    const long long r0 = static_cast<long long>(blockIdx.x) * kScanTile;
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) {
+        const int j = k * kScanThreads + tid;
+        s_row[scan_pad(j)] = r0 + j < m ? cnt[r0 + j] : 0;
+    }
+    __syncthreads();
+    long long base = 0;
+#pragma unroll
+    for (int i = 0; i < kScanThreads / kWarp; i++) base += s_before[i];
+    // thread tid: rows [tid * kScanPer, (tid + 1) * kScanPer) of the tile.
+    // int arithmetic inside the tile: it wraps only when the total leaves
+    // int32, which the plan's int64 total flags
+    int v[kScanPer];
+    int run = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) {
+        v[k] = s_row[scan_pad(tid * kScanPer + k)];
+        run += v[k];
+    }
+    const int inc = block_inclusive_scan<kScanThreads>(run, s_wtot);
+    int pos = static_cast<int>(base) + inc - run;
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) {
+        s_row[scan_pad(tid * kScanPer + k)] = pos;
+        pos += v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) {
+        const int j = k * kScanThreads + tid;
+        if (r0 + j < m) cnt[r0 + j] = s_row[scan_pad(j)];
+    }
+    if (blockIdx.x == gridDim.x - 1 && tid == 0) {
+        const long long total = base + s_wtot[kScanThreads / kWarp - 1];
+        cnt[m] = static_cast<int32_t>(total);
+        plan->total_key = total;
+        plan->overflow = total > INT32_MAX ? 1 : 0;
     }
 }
 
@@ -424,11 +679,37 @@ __global__ void k_total_nip(const int32_t* __restrict__ a_rpt, const int32_t* __
 
 cudaError_t launch_nip_hist(const int32_t* a_rpt, const int32_t* a_col, const int32_t* b_rpt,
                             int32_t m, int32_t* c_rpt, int32_t* nip_copy, int32_t* hist,
-                            Plan* plan, DevStatus* st, const Ladder& lad, cudaStream_t s) {
+                            Plan* plan, DevStatus* st, const Ladder& lad, cudaStream_t s,
+                            int32_t* hist_fill, int64_t* cta_sum, const Ladder* fill) {
     const int g = bin_ctas(m);
     if (g == 0) return cudaSuccess;
-    k_nip_hist<<<g, kBinThreads, 0, s>>>(a_rpt, a_col, b_rpt, m, c_rpt, nip_copy, hist, plan, st,
-                                         lad);
+    const Ladder none = {};
+    k_nip_hist<<<g, kNipThreads, 0, s>>>(a_rpt, a_col, b_rpt, m, c_rpt, nip_copy, hist, plan, st,
+                                         lad, fill != nullptr ? hist_fill : nullptr,
+                                         fill != nullptr ? cta_sum : nullptr,
+                                         fill != nullptr ? *fill : none);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bin_offsets_map(const int32_t* src_hist, int32_t* hist, int32_t nctas,
+                                   const Ladder& src, int64_t* cta_sum, Plan* plan,
+                                   const Ladder& lad, const Ladder* dlad, cudaStream_t s) {
+    k_bin_offsets_map<<<1, kOffMapThreads, 0, s>>>(src_hist, hist, nctas, src, cta_sum, plan, lad,
+                                                   dlad);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rpt_reduce(const int32_t* cnt, int32_t m, int64_t* tile_sum, Plan* plan,
+                              cudaStream_t s) {
+    if (m <= 0) return cudaSuccess;
+    k_rpt_reduce<<<rpt_scan_tiles(m), kScanThreads, 0, s>>>(cnt, m, tile_sum, plan);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rpt_scan(int32_t* cnt, int32_t m, const int64_t* tile_sum, Plan* plan,
+                            cudaStream_t s) {
+    if (m <= 0) return cudaSuccess;
+    k_rpt_scan<<<rpt_scan_tiles(m), kScanThreads, 0, s>>>(cnt, m, tile_sum, plan);
     return cudaGetLastError();
 }
 
@@ -448,11 +729,12 @@ cudaError_t launch_bin_offsets(int32_t* hist, int32_t nctas, int64_t* cta_sum, P
 
 cudaError_t launch_bin_scatter(int32_t* c_rpt, int32_t m, const int32_t* hist_off,
                                const int64_t* cta_off, int32_t* bins, const Plan* plan,
-                               const Ladder& lad, bool scan, cudaStream_t s, const Ladder* dlad) {
+                               const Ladder& lad, bool scan, cudaStream_t s, const Ladder* dlad,
+                               bool bin_relative) {
     const int g = bin_ctas(m);
     if (g == 0) return cudaSuccess;
     k_bin_scatter<<<g, kBinThreads, 0, s>>>(c_rpt, m, hist_off, cta_off, bins, plan, lad,
-                                            scan ? 1 : 0, dlad);
+                                            scan ? 1 : 0, dlad, bin_relative ? 1 : 0);
     return cudaGetLastError();
 }
 

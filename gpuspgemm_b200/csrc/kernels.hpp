@@ -98,8 +98,8 @@ constexpr int kBitmapCols = 1 << 20;
 constexpr int64_t kClusterBitmapCols = int64_t(8) * kBitmapCols;
 int s2n_bitmap_ladder_f64(const BinLauncher** out);
 int s2n_bitmap_ladder_f32(const BinLauncher** out);
-// One-pass ladder for B.n <= kBitmapCols (key = NIP of the row): the team bins
-// and the 256-thread bin expand, sort and compress; then the bitmap ladder's
+// One-pass ladder for B.n <= kBitmapCols (key = NIP of the row): the warp,
+// team and 256-thread bins expand, sort and compress; then the bitmap ladder's
 // bitmap and global bins.  Same bin count and limits as the bitmap ladder.
 int s2n_esc_ladder_f64(const BinLauncher** out);
 int s2n_esc_ladder_f32(const BinLauncher** out);
@@ -166,10 +166,22 @@ constexpr int kBinRowsPerCta = 1024;
 inline int bin_ctas(int32_t m) { return (m + kBinRowsPerCta - 1) / kBinRowsPerCta; }
 
 // Pass 1 (key = NIP): writes nip[r] into c_rpt[r] (and nip_copy[r] when not
-// nullptr), per-CTA bin histograms and the plan's total / max.
+// nullptr), per-CTA bin histograms and the plan's total / max.  With `fill`
+// given, also the per-CTA histograms by that ladder into hist_fill and the
+// per-CTA NIP sums into cta_sum (the fill binning's first pass).
 cudaError_t launch_nip_hist(const int32_t* a_rpt, const int32_t* a_col, const int32_t* b_rpt,
                             int32_t m, int32_t* c_rpt, int32_t* nip_copy, int32_t* hist,
-                            Plan* plan, DevStatus* st, const Ladder& lad, cudaStream_t s);
+                            Plan* plan, DevStatus* st, const Ladder& lad, cudaStream_t s,
+                            int32_t* hist_fill = nullptr, int64_t* cta_sum = nullptr,
+                            const Ladder* fill = nullptr);
+// Pass 2 for histograms src_hist counted by a source ladder `src` whose
+// limits include every limit of the final ladder (dlad when given, else lad):
+// the outputs of launch_bin_offsets for the final ladder, all bins at once,
+// except that hist (another array) receives offsets within each bin: the
+// scatter that reads them is launched with bin_relative.
+cudaError_t launch_bin_offsets_map(const int32_t* src_hist, int32_t* hist, int32_t nctas,
+                                   const Ladder& src, int64_t* cta_sum, Plan* plan,
+                                   const Ladder& lad, const Ladder* dlad, cudaStream_t s);
 // Pass 1' (key = nnz already in c_rpt): per-CTA sums and bin histograms.
 // dlad: limits chosen on the device (same bin count as lad), or nullptr.
 cudaError_t launch_nnz_hist(const int32_t* c_rpt, int32_t m, int32_t* hist, int64_t* cta_sum,
@@ -184,7 +196,19 @@ cudaError_t launch_bin_offsets(int32_t* hist, int32_t nctas, int64_t* cta_sum, P
 cudaError_t launch_bin_scatter(int32_t* c_rpt, int32_t m, const int32_t* hist_off,
                                const int64_t* cta_off, int32_t* bins, const Plan* plan,
                                const Ladder& lad, bool scan, cudaStream_t s,
-                               const Ladder* dlad = nullptr);
+                               const Ladder* dlad = nullptr, bool bin_relative = false);
+// One-pass row pointer: rewrite cnt[0..m) (each row's nnz) as its exclusive
+// scan and cnt[m] as the total, in place; the plan (zeroed by the caller)
+// receives the total, the max and the int32 overflow flag.  tile_sum holds
+// rpt_scan_tiles(m) sums.  Only for rpt_scan_tiles(m) <= kScanMaxTiles (each
+// CTA adds up the tiles before its own).
+constexpr int kScanTile = 4096;
+constexpr int kScanMaxTiles = 2048;
+inline int rpt_scan_tiles(int32_t m) { return (m + kScanTile - 1) / kScanTile; }
+cudaError_t launch_rpt_reduce(const int32_t* cnt, int32_t m, int64_t* tile_sum, Plan* plan,
+                              cudaStream_t s);
+cudaError_t launch_rpt_scan(int32_t* cnt, int32_t m, const int64_t* tile_sum, Plan* plan,
+                            cudaStream_t s);
 // One-pass fill: copy each row's entries from its slot [off[r], ...) of the
 // temporary arrays to [rpt[r], rpt[r+1]) of C (values of value_bytes 4 or 8).
 cudaError_t launch_compact_rows(const int32_t* off, const int32_t* rpt, int32_t m,

@@ -60,6 +60,7 @@ struct Scratch {
     Plan* plan2;
     int32_t* hist1;
     int32_t* hist2;
+    int32_t* hist3;  // the NIP pass's fill-ladder counts (early one-pass products)
     int64_t* cta_sum;
     int32_t* bins1;
     int32_t* bins2;
@@ -192,6 +193,7 @@ spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s, cudaStre
     const size_t o_dladder = take(sizeof(Ladder));
     const size_t o_hist1 = take(sizeof(int32_t) * kMaxBins * nctas);
     const size_t o_hist2 = take(sizeof(int32_t) * kMaxBins * nctas);
+    const size_t o_hist3 = take(sizeof(int32_t) * kMaxBins * nctas);
     const size_t o_sum = take(sizeof(int64_t) * nctas);
     const size_t o_bins1 = take(sizeof(int32_t) * mm);
     const size_t o_bins2 = take(sizeof(int32_t) * mm);
@@ -209,6 +211,7 @@ spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s, cudaStre
     s->dladder = reinterpret_cast<Ladder*>(b + o_dladder);
     s->hist1 = reinterpret_cast<int32_t*>(b + o_hist1);
     s->hist2 = reinterpret_cast<int32_t*>(b + o_hist2);
+    s->hist3 = reinterpret_cast<int32_t*>(b + o_hist3);
     s->cta_sum = reinterpret_cast<int64_t*>(b + o_sum);
     s->bins1 = reinterpret_cast<int32_t*>(b + o_bins1);
     s->bins2 = reinterpret_cast<int32_t*>(b + o_bins2);
@@ -578,16 +581,50 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         off = static_cast<int32_t*>(h->slots);
         off_written = true;
     }
-    B200_STEP(timed(h, "nip_hist", 0, -1, m, stream, [&](cudaStream_t ss) {
-        return launch_nip_hist(A->rpt, A->col, B->rpt, m, c_rpt, off, s.hist1, s.plan1, s.status,
-                               lad1, ss);
-    }));
     // The fill binning by NIP (the one-pass path's), with limits decided on
     // the device when the sample ran: off = the scan of the NIP per row.
     Ladder ladh = ladf;
     if (esc_mode == 1) ladh.limit[kEscBins - 1] = kEscSplit;
     const Ladder* dlad = sampled ? s.dladder : nullptr;
+    // Early products: the NIP pass also counts the rows by the fill ladder's
+    // limits plus the split the device may choose (the sample runs beside
+    // it), and the fill binning maps those counts onto the chosen ladder.
+    Ladder ladx = ladh;
+    ladx.min_bin = 0;  // the mapping applies the chosen ladder's
+    bool ladx_ok = true;
+    if (sampled) {
+        int pos = 0;
+        while (pos < ladx.nb && ladx.limit[pos] < kEscSplit) pos++;
+        if (pos == ladx.nb || ladx.limit[pos] != kEscSplit) {
+            if (ladx.nb < kMaxBins) {
+                for (int i = ladx.nb; i > pos; i--) ladx.limit[i] = ladx.limit[i - 1];
+                ladx.limit[pos] = kEscSplit;
+                ladx.nb++;
+            } else {
+                ladx_ok = false;  // no room: the fill binning counts the rows itself
+            }
+        }
+    }
+    const bool nip_counts_fill = early && ladx_ok;
+    B200_STEP(timed(h, "nip_hist", 0, -1, m, stream, [&](cudaStream_t ss) {
+        return launch_nip_hist(A->rpt, A->col, B->rpt, m, c_rpt, off, s.hist1, s.plan1, s.status,
+                               lad1, ss, s.hist3, s.cta_sum, nip_counts_fill ? &ladx : nullptr);
+    }));
     auto fill_binning = [&]() -> spgemm_status {
+        if (nip_counts_fill) {
+            // the NIP pass counted the rows by ladx: offsets for the chosen
+            // ladder, then the scatter
+            if (sampled) B200_TRY(cudaStreamWaitEvent(stream, h->ev_sample, 0));
+            B200_STEP_R(timed(h, "nip_fill_offsets", 2, -1, m, stream, [&](cudaStream_t ss) {
+                return launch_bin_offsets_map(s.hist3, s.hist2, nctas, ladx, s.cta_sum, s.plan2,
+                                              ladh, dlad, ss);
+            }));
+            B200_STEP_R(timed(h, "nip_fill_scatter", 2, -1, m, stream, [&](cudaStream_t ss) {
+                return launch_bin_scatter(off, m, s.hist2, s.cta_sum, s.bins2, s.plan2, ladh, true,
+                                          ss, dlad, true);
+            }));
+            return SPGEMM_OK;
+        }
         if (!off_written) {
             B200_STEP_R(regrow(h, &h->slots, &h->slots_bytes, sizeof(int32_t) * (size_t(m) + 1),
                                stream));
@@ -772,22 +809,32 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         }
         mark(4);
         B200_ONE(launch_bins(h, one_fil, nfil, 3, pf, s.bins2, pa, stream));
-        // row pointer from the counts: a one-bin pass with the scan, into the
-        // count binning's plan (reset: its max and overflow only ever grow)
+        // row pointer from the counts, into the count binning's plan (reset:
+        // its max and overflow only ever grow): reduce, then scan -- or, past
+        // the scan's tile limit, a one-bin pass of the binning kernels
         B200_ONE_CUDA(cudaMemsetAsync(s.plan1, 0, sizeof(Plan), stream), "reset a plan");
-        Ladder one = {};
-        one.nb = 1;
-        one.limit[0] = INT32_MAX;
-        B200_ONE(timed(h, "count_scan_hist", 2, -1, m, stream, [&](cudaStream_t ss) {
-            return launch_nnz_hist(c_rpt, m, s.hist1, s.cta_sum, s.plan1, one, ss);
-        }));
-        B200_ONE(timed(h, "count_scan_offsets", 2, -1, m, stream, [&](cudaStream_t ss) {
-            return launch_bin_offsets(s.hist1, nctas, s.cta_sum, s.plan1, one, ss);
-        }));
-        B200_ONE(timed(h, "count_scan_scatter", 2, -1, m, stream, [&](cudaStream_t ss) {
-            return launch_bin_scatter(c_rpt, m, s.hist1, s.cta_sum, s.bins1, s.plan1, one, true,
-                                      ss);
-        }));
+        if (rpt_scan_tiles(m) <= kScanMaxTiles) {
+            B200_ONE(timed(h, "count_scan_reduce", 2, -1, m, stream, [&](cudaStream_t ss) {
+                return launch_rpt_reduce(c_rpt, m, s.cta_sum, s.plan1, ss);
+            }));
+            B200_ONE(timed(h, "count_scan_rows", 2, -1, m, stream, [&](cudaStream_t ss) {
+                return launch_rpt_scan(c_rpt, m, s.cta_sum, s.plan1, ss);
+            }));
+        } else {
+            Ladder one = {};
+            one.nb = 1;
+            one.limit[0] = INT32_MAX;
+            B200_ONE(timed(h, "count_scan_hist", 2, -1, m, stream, [&](cudaStream_t ss) {
+                return launch_nnz_hist(c_rpt, m, s.hist1, s.cta_sum, s.plan1, one, ss);
+            }));
+            B200_ONE(timed(h, "count_scan_offsets", 2, -1, m, stream, [&](cudaStream_t ss) {
+                return launch_bin_offsets(s.hist1, nctas, s.cta_sum, s.plan1, one, ss);
+            }));
+            B200_ONE(timed(h, "count_scan_scatter", 2, -1, m, stream, [&](cudaStream_t ss) {
+                return launch_bin_scatter(c_rpt, m, s.hist1, s.cta_sum, s.bins1, s.plan1, one,
+                                          true, ss);
+            }));
+        }
         mark(5);
         B200_ONE(sync_mirror(h, stream, s.plan1, s));
         B200_ONE(status_to_error(h->mirror->status));
