@@ -42,8 +42,8 @@ FALLBACK_HBM_GBS = 6650.0
 # (`-k <kernel> -c 1`, cold caches): key (kernel, value dtype).  Other
 # workloads report traffic null.
 MEASURED_TRAFFIC = {
-    ("s2n_bitmap1024", "f64"): 85_622_272 + 69_268_480,
-    ("esc_cta256_n3072", "f64"): 80_557_824 + 65_419_264,
+    ("s2n_bitmap1024", "f64"): 85_734_144 + 69_866_240,
+    ("esc_cta256_n3072", "f64"): 80_353_792 + 66_175_744,
 }
 
 
@@ -164,13 +164,25 @@ def replica_gflops(nip: int, steps: int, world: int, max_ms: float) -> float:
 
 # ---- clocks -----------------------------------------------------------------
 
+def nvml_early_init() -> None:
+    """Initialise NVML once, before any timed work: its first initialisation
+    runs for a while in the driver, and the clock readers below would
+    otherwise pay it at the start of a timed region."""
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+    except Exception:
+        pass
+
+
 class ClockSampler:
     """SM clock and clock-event reasons sampled DURING a timed region: NVML
-    polled every 25 ms from a thread; nvidia-smi at its 200 ms minimum if NVML
-    is unavailable.  Polling every 5 ms stalled about one product in 50 by
-    ~1 ms on a B200 (each poll's driver calls contend with the product's own
-    synchronisations), which moved the plain product's mean by 2 %; at 25 ms
-    the timed region of 100 products still sees several samples.
+    polled every 25 ms from a thread, or -- `between_steps` -- read by the
+    timing loop itself between two steps of the region (tick()); nvidia-smi at
+    its 200 ms minimum if NVML is unavailable.  A polling thread stalled about
+    one plain product in 50 by ~1 ms on a B200, at 5 ms and at 25 ms alike (its
+    driver calls contend with the product's own synchronisations), moving the
+    mean by 1-2 %; reads between steps overlap no product.
     Reads only -- no setting of the GPU is touched."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -180,8 +192,10 @@ class ClockSampler:
                "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
                "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, between_steps: bool = False):
         self.gpu = gpu_index
+        self.between_steps = between_steps
+        self.hd = None
         self.proc = None
         self.lines = []
         self.samples = []  # (sm MHz, max MHz, reason bits) from NVML
@@ -210,10 +224,26 @@ class ClockSampler:
                 pass
             self.stop.wait(0.025)
 
+    def tick(self):
+        """One reading, from the timing loop between two steps."""
+        if self.nvml is None or not self.between_steps:
+            return
+        try:
+            nv, hd = self.nvml, self.hd
+            self.samples.append((float(nv.nvmlDeviceGetClockInfo(hd, nv.NVML_CLOCK_SM)),
+                                 float(self.max_mhz),
+                                 int(nv.nvmlDeviceGetCurrentClocksEventReasons(hd))))
+        except Exception:
+            pass
+
     def __enter__(self):
         try:
             nv, hd = self._nvml_handle()
             self.nvml = nv
+            if self.between_steps:
+                self.hd = hd
+                self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(hd, nv.NVML_CLOCK_SM)
+                return self
             self.t = threading.Thread(target=self._poll, args=(nv, hd), daemon=True)
             self.t.start()
             t0 = time.perf_counter()  # polling before the region starts
@@ -239,6 +269,8 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        if self.nvml is not None and self.between_steps:
+            return
         if self.nvml is not None:
             self.stop.set()
             self.t.join(timeout=2)
@@ -259,7 +291,7 @@ class ClockSampler:
                 for nm, const in self.REASONS.items():
                     if bits & int(getattr(self.nvml, const, 0)):
                         reasons.add(nm)
-            source = "nvml, 25 ms"
+            source = "nvml, between steps" if self.between_steps else "nvml, 25 ms"
         else:
             names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
             for ln in self.lines:
@@ -355,13 +387,15 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clk:
+    with ClockSampler(local_rank, between_steps=True) as clk:
         for i in range(args.steps):
             flush.fill_(float(i))
             starts[i].record(stream)
             C = proposal(dA, dA, h)
             ends[i].record(stream)
             del C
+            if i % 10 == 0:
+                clk.tick()  # the call has returned: no product in flight
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -529,7 +563,8 @@ def run_ours(args, rank, world, local_rank):
         "metric": metric_name(args.dtype), "value": value, "unit": "GFLOPS", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "step_ms": {"min": float(np.min(step_ms)), "median": float(np.median(step_ms)),
-                    "max": float(np.max(step_ms)), "first": float(step_ms[0])},
+                    "max": float(np.max(step_ms)), "max_at": int(np.argmax(step_ms)),
+                    "first": float(step_ms[0])},
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": args.dtype, "data": "synthetic (seeded generator)",
         "config": config_of(args, A, nip, nnz_c),
@@ -677,8 +712,9 @@ def run_galerkin(args, local_rank):
     # the chain as one call (inputs of 300+ MB: larger than L2), and its stages
     t_call, t_tr, t_ap, t_rap = [], [], [], []
     torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clk:
+    with ClockSampler(local_rank, between_steps=True) as clk:
         for _ in range(args.steps):
+            clk.tick()  # between steps: no product in flight
             e = [ev() for _ in range(5)]
             e[0].record(stream)
             C = rap(A, P, None, h)
@@ -909,6 +945,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "ours":
+        nvml_early_init()
     if args.mode == "batch":
         line = run_batch(args, local_rank) if rank == 0 else None
     elif args.mode == "served":

@@ -579,7 +579,7 @@ template<typename W>
 __global__ __launch_bounds__(kCompactThreads) void k_compact_rows(
     const int32_t* __restrict__ off, const int32_t* __restrict__ rpt, int32_t m,
     const int32_t* __restrict__ tmp_col, const W* __restrict__ tmp_val,
-    int32_t* __restrict__ col, W* __restrict__ val) {
+    int32_t* __restrict__ col, W* __restrict__ val, int32_t cap) {
     constexpr int NW = kCompactThreads / kWarp;
     constexpr int U = kCompactUnroll;
     __shared__ int32_t s_rpt[kCompactRows + 1];
@@ -592,7 +592,7 @@ __global__ __launch_bounds__(kCompactThreads) void k_compact_rows(
     }
     __syncthreads();
     const int j0 = s_rpt[0];
-    const int j1 = s_rpt[nr];
+    const int j1 = min(s_rpt[nr], cap);  // a count past C's capacity is reported by the host
     const bool step = (j1 - j0) >= kCompactStepMin * nr;  // uniform over the CTA
     // the last row i of the chunk with s_rpt[i] <= j
     auto search = [&](int j) {
@@ -740,17 +740,17 @@ cudaError_t launch_bin_scatter(int32_t* c_rpt, int32_t m, const int32_t* hist_of
 
 cudaError_t launch_compact_rows(const int32_t* off, const int32_t* rpt, int32_t m,
                                 const int32_t* tmp_col, const void* tmp_val, int32_t* col,
-                                void* val, int value_bytes, cudaStream_t s) {
+                                void* val, int value_bytes, cudaStream_t s, int32_t cap) {
     if (m <= 0) return cudaSuccess;
     const int g = (m + kCompactRows - 1) / kCompactRows;
     if (value_bytes == 8)
         k_compact_rows<long long><<<g, kCompactThreads, 0, s>>>(
             off, rpt, m, tmp_col, static_cast<const long long*>(tmp_val), col,
-            static_cast<long long*>(val));
+            static_cast<long long*>(val), cap);
     else
         k_compact_rows<int32_t><<<g, kCompactThreads, 0, s>>>(
             off, rpt, m, tmp_col, static_cast<const int32_t*>(tmp_val), col,
-            static_cast<int32_t*>(val));
+            static_cast<int32_t*>(val), cap);
     return cudaGetLastError();
 }
 

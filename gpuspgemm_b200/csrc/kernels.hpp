@@ -210,10 +210,15 @@ cudaError_t launch_rpt_reduce(const int32_t* cnt, int32_t m, int64_t* tile_sum, 
 cudaError_t launch_rpt_scan(int32_t* cnt, int32_t m, const int64_t* tile_sum, Plan* plan,
                             cudaStream_t s);
 // One-pass fill: copy each row's entries from its slot [off[r], ...) of the
-// temporary arrays to [rpt[r], rpt[r+1]) of C (values of value_bytes 4 or 8).
+// temporary arrays to [rpt[r], rpt[r+1]) of C (values of value_bytes 4 or 8);
+// nothing at or past `cap`, C's capacity.
 cudaError_t launch_compact_rows(const int32_t* off, const int32_t* rpt, int32_t m,
                                 const int32_t* tmp_col, const void* tmp_val, int32_t* col,
-                                void* val, int value_bytes, cudaStream_t s);
+                                void* val, int value_bytes, cudaStream_t s, int32_t cap);
+// A one-pass C gets the product's NIP as its capacity before its nnz is known
+// when the sampled rows' NIP / nnz is at most this; a C with more spare
+// capacity than this factor is then copied to arrays of its size.
+constexpr double kCapSlack = 1.1;
 // Operand validation (checked mode).
 cudaError_t launch_check_csr(const int32_t* rpt, const int32_t* col, int32_t m, int32_t n,
                              int32_t nnz, DevStatus* st, cudaStream_t s);

@@ -836,6 +836,82 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
             }));
         }
         mark(5);
+        // Products whose sampled rows repeat few columns give C the NIP as
+        // its capacity right away, so the compaction follows the scan with
+        // no host round trip; a C that turns out more than kCapSlack
+        // smaller is copied to arrays of its size after the last
+        // synchronisation.  Others size C exactly, from the scan.
+        const bool c_by_nip = sampled && team_nnz > 0 &&
+                              static_cast<double>(team_nip) <=
+                                  kCapSlack * static_cast<double>(team_nnz);
+        if (c_by_nip) {
+            B200_ONE_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&C->col),
+                                                  sizeof(int32_t) * size_t(nip_total) + 16,
+                                                  h->pool, stream),
+                          "allocate C.col");
+            B200_ONE_CUDA(cudaMallocFromPoolAsync(&C->val, sizeof(V) * size_t(nip_total),
+                                                  h->pool, stream),
+                          "allocate C.val");
+            B200_ONE(timed(h, "compact_rows", 3, -1, m, stream, [&](cudaStream_t ss) {
+                return launch_compact_rows(off, c_rpt, m, tmp_col, tmp_val, C->col, C->val,
+                                           static_cast<int>(sizeof(V)), ss,
+                                           static_cast<int32_t>(nip_total));
+            }));
+            release();
+            auto drop_c = [&]() {
+                (void)cudaFreeAsync(C->col, stream);
+                (void)cudaFreeAsync(C->val, stream);
+                C->col = nullptr;
+                C->val = nullptr;
+            };
+            if (spgemm_status st = sync_mirror(h, stream, s.plan1, s); st != SPGEMM_OK)
+                return drop_c(), bail(st);
+            if (spgemm_status st = status_to_error(h->mirror->status); st != SPGEMM_OK)
+                return drop_c(), bail(st);
+            const Plan pc = h->mirror->plan;
+            if (pc.overflow || pc.total_key > nip_total)
+                return drop_c(),
+                       bail(fail(SPGEMM_ERR_INTERNAL, "one-pass row counts out of range"));
+            const int32_t nnz = static_cast<int32_t>(pc.total_key);
+            h->info.nnz = nnz;
+            h->info.max_row_nnz = pc.max_key;
+            C->nnz = nnz;
+            bool resized = false;
+            if (nnz == 0) {
+                drop_c();
+            } else if (static_cast<double>(nnz) * kCapSlack < static_cast<double>(nip_total)) {
+                resized = true;
+                // more spare capacity than the slack: arrays of C's size
+                int32_t* col = nullptr;
+                void* val = nullptr;
+                cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&col),
+                                                        sizeof(int32_t) * size_t(nnz) + 16,
+                                                        h->pool, stream);
+                if (e == cudaSuccess)
+                    e = cudaMallocFromPoolAsync(&val, sizeof(V) * size_t(nnz), h->pool, stream);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(col, C->col, sizeof(int32_t) * size_t(nnz),
+                                        cudaMemcpyDeviceToDevice, stream);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(val, C->val, sizeof(V) * size_t(nnz),
+                                        cudaMemcpyDeviceToDevice, stream);
+                drop_c();
+                C->col = col;
+                C->val = val;
+                if (e != cudaSuccess) {
+                    drop_c();
+                    return bail(cuda_fail(e, "size C"));
+                }
+            }
+            if (resized) {
+                if (cudaError_t e = cudaStreamSynchronize(stream); e != cudaSuccess)
+                    return bail(cuda_fail(e, "final synchronize"));
+                h->info.host_syncs++;
+            }
+            mark(6);
+            resolve_profile(h);
+            return SPGEMM_OK;
+        }
         B200_ONE(sync_mirror(h, stream, s.plan1, s));
         B200_ONE(status_to_error(h->mirror->status));
         const Plan pc = h->mirror->plan;
@@ -855,7 +931,7 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
                           "allocate C.val");
             B200_ONE(timed(h, "compact_rows", 3, -1, m, stream, [&](cudaStream_t ss) {
                 return launch_compact_rows(off, c_rpt, m, tmp_col, tmp_val, C->col, C->val,
-                                           static_cast<int>(sizeof(V)), ss);
+                                           static_cast<int>(sizeof(V)), ss, nnz);
             }));
         }
         release();

@@ -419,12 +419,41 @@ def test_one_pass_chosen_and_equal_to_two_pass(handle, oracle_mod):
         info2 = handle.info()
     finally:
         handle.set_option(N.OPT_ONE_PASS, 0)
-    # one pass, binned for the fill before the first synchronisation: NIP +
-    # fill binning, row counts, final; two passes: NIP binning, scan, final
-    assert info2["one_pass"] == 0 and info2["host_syncs"] == 3 and info1["host_syncs"] == 3
+    # one pass, binned for the fill before the first synchronisation, and C
+    # given the NIP as capacity (the sample sees few repeated columns): NIP +
+    # fill binning, final; two passes: NIP binning, scan, final
+    assert info2["one_pass"] == 0 and info2["host_syncs"] == 3 and info1["host_syncs"] == 2
     assert np.array_equal(C1.rpt, C2.rpt) and np.array_equal(C1.col, C2.col)
     assert info1["nnz"] == info2["nnz"] and info1["max_row_nnz"] == info2["max_row_nnz"]
     check(oracle_mod, A, A, C1, np.float64, "one_pass_default", positive=True)
+
+
+def test_one_pass_capacity_shrinks_to_nnz(handle, oracle_mod):
+    """A one-pass product whose sampled (light) rows repeat no column gets the
+    NIP as C's capacity before its nnz is known; here the heavy rows collapse
+    onto ten columns, so nnz is far below the NIP and C is copied to arrays of
+    its own size after the last synchronisation (one more): the result still
+    equals the oracle's."""
+    rng = np.random.default_rng(31)
+    n = 1 << 20
+    clones, distinct = 2000, 200000
+    b_rows = [np.arange(10, dtype=np.int32)] * clones
+    b_rows += [np.sort(rng.choice(n, 5, replace=False)).astype(np.int32) for _ in range(distinct)]
+    b_rpt = np.concatenate([[0], np.cumsum([len(r) for r in b_rows])]).astype(np.int32)
+    B = HostCSR(len(b_rows), n, b_rpt, np.concatenate(b_rows),
+                rng.uniform(0.5, 1.0, int(b_rpt[-1])))
+    light = [np.sort(clones + rng.choice(distinct, 2, replace=False)).astype(np.int32)
+             for _ in range(200000)]
+    heavy = [np.sort(rng.choice(clones, 150, replace=False)).astype(np.int32) for _ in range(3000)]
+    a_rows = light + heavy
+    a_rpt = np.concatenate([[0], np.cumsum([len(r) for r in a_rows])]).astype(np.int32)
+    A = HostCSR(len(a_rows), B.m, a_rpt, np.concatenate(a_rows),
+                rng.uniform(0.5, 1.0, int(a_rpt[-1])))
+    C = gpu_product(A, B, handle, np.float64)
+    info = handle.info()
+    assert info["one_pass"] == 1 and info["nip"] > 2 * info["nnz"]
+    assert info["host_syncs"] == 3  # NIP + fill binning, row counts, the copy to C's size
+    check(oracle_mod, A, B, C, np.float64, "one_pass_capacity_shrink", positive=True)
 
 
 def test_heavy_row_spills_to_global(handle, oracle_mod):
