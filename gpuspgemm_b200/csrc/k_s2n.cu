@@ -747,14 +747,17 @@ __global__ __launch_bounds__(THREADS) void k_s2n_cta(ProductArgs p) {
 // The kernel is persistent: one CTA per SM (the bitmap takes most of its
 // shared memory) clears the bitmap once and then takes rows blockIdx.x,
 // blockIdx.x + gridDim.x, ...  Thread t owns summary word t, i.e. bitmap
-// words [32t, 32t + 32) = four 8-word blocks.  Per row: fill; each thread
+// words [32t, 32t + 32) = eight 4-word blocks.  Per row: fill; each thread
 // counts the set bits of its non-empty words; a block scan gives every
 // thread's first position, from which it writes its columns to C.col and
 // records the rank of each of its blocks' first bit.  The bitmap stays
 // intact, so a key's position in the row is its rank -- the block's rank plus
-// the set bits before it in at most 8 words, all independent reads --
+// the set bits before it in at most 4 words, all independent reads --
 // instead of a binary search; values accumulate with global reductions into
 // C.val.  Then each thread clears its non-empty words and summary word.
+// (4-word blocks rather than 8: 0.289 -> 0.280 ms on the 1M power-law
+// product, for 16 KB more shared memory.)  The cluster bin below keeps
+// 8-word blocks in the same layout (its rank table uses half the space).
 constexpr int kBitmapWords = kBitmapCols / 32;
 constexpr int kSummaryWords = kBitmapWords / 32;
 
@@ -762,7 +765,7 @@ template<typename V, int THREADS, int CAP>
 struct BitmapLayout {
     static constexpr size_t bm_bytes = sizeof(uint32_t) * kBitmapWords;
     static constexpr size_t summary_bytes = sizeof(uint32_t) * kSummaryWords;
-    static constexpr size_t rank_bytes = sizeof(int32_t) * (kBitmapWords / 8);
+    static constexpr size_t rank_bytes = sizeof(int32_t) * (kBitmapWords / 4);
     static constexpr size_t bytes =
         bm_bytes + summary_bytes + rank_bytes + sizeof(CtaScratch<THREADS>);
     static_assert(kSummaryWords == THREADS, "one summary word per thread");
@@ -829,10 +832,10 @@ __global__ __launch_bounds__(THREADS) void k_s2n_bitmap(ProductArgs p) {
         int pos = inc - cnt;
         int32_t* cols = p.c_col + c0;
 #pragma unroll
-        for (int bb = 0; bb < 4; bb++) {
-            block_rank[(w0 >> 3) + bb] = pos;
-            for (uint32_t m = (sw >> (8 * bb)) & 0xffu; m != 0u; m &= m - 1u) {
-                const int wi = w0 + 8 * bb + __ffs(m) - 1;
+        for (int bb = 0; bb < 8; bb++) {
+            block_rank[(w0 >> 2) + bb] = pos;
+            for (uint32_t m = (sw >> (4 * bb)) & 0xfu; m != 0u; m &= m - 1u) {
+                const int wi = w0 + 4 * bb + __ffs(m) - 1;
                 for (uint32_t word = bm[wi]; word != 0u; word &= word - 1u) {
                     if (pos < bound) cols[pos] = wi * 32 + __ffs(word) - 1;
                     pos++;
@@ -858,11 +861,11 @@ __global__ __launch_bounds__(THREADS) void k_s2n_bitmap(ProductArgs p) {
                 const int32_t key = kp.key;
                 if (static_cast<uint32_t>(key) >= static_cast<uint32_t>(p.n_cols)) return;
                 const int wi = key >> 5;
-                const int w8 = wi & ~7;
-                int rank = block_rank[wi >> 3] + __popc(bm[wi] & ((1u << (key & 31)) - 1u));
+                const int w4 = wi & ~3;
+                int rank = block_rank[wi >> 2] + __popc(bm[wi] & ((1u << (key & 31)) - 1u));
 #pragma unroll
-                for (int t = 0; t < 7; t++)
-                    if (w8 + t < wi) rank += __popc(bm[w8 + t]);
+                for (int t = 0; t < 3; t++)
+                    if (w4 + t < wi) rank += __popc(bm[w4 + t]);
                 if (rank < nnz) atomicAdd(out + rank, kp.prod);
             });
         for (uint32_t m = sw; m != 0u; m &= m - 1u) bm[w0 + __ffs(m) - 1] = 0u;
