@@ -859,6 +859,8 @@ def run_served(args, local_rank):
             lat.append(_t.perf_counter() - t_start - ta)
         return np.array(lat), _t.perf_counter() - t_start
 
+    spans = []  # every served run's unit summary, in order
+
     def served(arrivals):
         kw = {}
         if args.solo_nip is not None:
@@ -880,9 +882,20 @@ def run_served(args, local_rank):
         for r in reqs:  # keep the timings, free the results before the next run
             r.result = None
         tl = server.timeline
+        busy = {}
+        for wid, _, t_adm, t_launch, t_done in tl:
+            busy[wid] = busy.get(wid, 0.0) + (t_done - t_launch)
         batches = {"units": len(tl), "batched": sum(1 for u in tl if u[1] > 1),
                    "alone": sum(1 for u in tl if u[1] == 1),
-                   "largest_batch": max((u[1] for u in tl), default=0)}
+                   "largest_batch": max((u[1] for u in tl), default=0),
+                   "span_ms": span * 1e3,
+                   "worker_busy_ms": [round(busy.get(w, 0.0) * 1e3, 1) for w in range(workers)],
+                   "pack_ms": round(sum(u[3] - u[2] for u in tl) * 1e3, 1),
+                   "unit_ms_max": round(max((u[4] - u[3] for u in tl), default=0.0) * 1e3, 2),
+                   # the five longest units: (requests, ms, launched at ms, worker)
+                   "slowest": [(u[1], round((u[4] - u[3]) * 1e3, 2), round((u[3] - t_start) * 1e3, 1),
+                                u[0]) for u in sorted(tl, key=lambda u: u[3] - u[4])[:5]]}
+        spans.append(batches)
         server.close()
         if bad:
             raise bad[0].error
@@ -894,7 +907,9 @@ def run_served(args, local_rank):
 
     # saturation: every request present at t = 0 (median of 3 runs each)
     zero = np.zeros(len(picks))
-    served(zero[: min(32, len(picks))])  # warm the server's handles
+    # warm-up: one whole untimed run (the first run grows the device's memory
+    # pool and the workers' scratch: its units ran up to 7x longer)
+    served(zero)
     reqs_sat, span_sat, batches_sat = median_run(lambda: served(zero), key=lambda r: r[1])
     _, span_plain_sat = median_run(lambda: plain_fifo(zero), key=lambda r: r[1])
     # fixed offered load: Poisson arrivals at `load` x the plain path's capacity;
@@ -930,7 +945,8 @@ def run_served(args, local_rank):
                        "plain_products_per_s": len(picks) / span_plain_sat,
                        "speedup": span_plain_sat / span_sat,
                        "served_gflops": 2.0 * total_nip / span_sat / 1e9,
-                       "batches": batches_sat},
+                       "batches": batches_sat,
+                       "runs": spans[1:4]},
         "at_load": {"offered_per_s": rate, "served": s_load, "served_by_kind": by_kind,
                     "plain_fifo_by_kind": plain_by_kind,
                     "plain_fifo": {"p50_ms": float(np.percentile(lat_plain, 50) * 1e3),
