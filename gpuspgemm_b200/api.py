@@ -303,20 +303,55 @@ def pack_batch(pairs) -> PackedBatch:
 
 
 def _batch_views(out: N.BatchOut, dtype) -> list[DeviceCSR]:
+    """One DeviceCSR per product, as views into the batch's device arrays.
+    Products of one group lie one after another in three arrays (row
+    pointers, columns, values): each run of such products is wrapped once per
+    array and sliced per product -- a tensor slice costs a few microseconds,
+    wrapping an array through __cuda_array_interface__ tens, which a batch of
+    fifty small products paid 150 times."""
     owner = _BatchOwner(out)
     dev = torch.device("cuda", torch.cuda.current_device())
     vt = "<f8" if dtype == torch.float64 else "<f4"
+    vsz = 8 if dtype == torch.float64 else 4
+    P = out.products
+    count = out.count
     res = []
-    for i in range(out.count):
-        p = out.products[i]
-        rpt = torch.as_tensor(_LibraryArray(owner, p.rpt, p.m + 1, "<i4"), device=dev)
-        if p.nnz > 0:
-            col = torch.as_tensor(_LibraryArray(owner, p.col, p.nnz, "<i4"), device=dev)
-            val = torch.as_tensor(_LibraryArray(owner, p.val, p.nnz, vt), device=dev)
-        else:
-            col = torch.empty(0, dtype=torch.int32, device=dev)
-            val = torch.empty(0, dtype=dtype, device=dev)
-        res.append(DeviceCSR(int(p.m), int(p.n), rpt, col, val))
+    i = 0
+    while i < count:
+        first = P[i]
+        # the run: row pointers back to back, and (products with entries)
+        # columns and values back to back
+        j = i + 1
+        rlen = first.m + 1
+        clen = first.nnz
+        if first.nnz > 0:
+            while j < count:
+                a, b = P[j - 1], P[j]
+                if (b.nnz == 0 or b.rpt != a.rpt + 4 * (a.m + 1) or
+                        b.col != a.col + 4 * a.nnz or b.val != a.val + vsz * a.nnz):
+                    break
+                rlen += b.m + 1
+                clen += b.nnz
+                j += 1
+        rpt_all = torch.as_tensor(_LibraryArray(owner, first.rpt, rlen, "<i4"), device=dev)
+        if clen > 0:
+            col_all = torch.as_tensor(_LibraryArray(owner, first.col, clen, "<i4"), device=dev)
+            val_all = torch.as_tensor(_LibraryArray(owner, first.val, clen, vt), device=dev)
+        ro = 0
+        co = 0
+        for k in range(i, j):
+            p = P[k]
+            rpt = rpt_all[ro:ro + p.m + 1]
+            ro += p.m + 1
+            if p.nnz > 0:
+                col = col_all[co:co + p.nnz]
+                val = val_all[co:co + p.nnz]
+                co += p.nnz
+            else:
+                col = torch.empty(0, dtype=torch.int32, device=dev)
+                val = torch.empty(0, dtype=dtype, device=dev)
+            res.append(DeviceCSR(int(p.m), int(p.n), rpt, col, val))
+        i = j
     return res
 
 
