@@ -42,7 +42,7 @@ FALLBACK_HBM_GBS = 6650.0
 # (`-k <kernel> -c 1`, cold caches): key (kernel, value dtype).  Other
 # workloads report traffic null.
 MEASURED_TRAFFIC = {
-    ("s2n_bitmap1024", "f64"): 85_734_144 + 69_866_240,
+    ("s2n_bitmap1024", "f64"): 85_709_056 + 69_113_088,
     ("esc_cta256_n3072", "f64"): 80_353_792 + 66_175_744,
 }
 
@@ -905,6 +905,23 @@ def run_served(args, local_rank):
         runs = sorted((fn() for _ in range(3)), key=key)
         return runs[1]
 
+    # Python's cyclic garbage collector stops every thread while it walks the
+    # heap: a full collection over the request pool's objects paused all four
+    # workers for ~56 ms in one run.  Long-lived objects go to the permanent
+    # generation first, as a latency-sensitive Python server would do.
+    import gc
+    gc_log = []  # (generation, seconds) of every collection during the runs
+    gc_t0 = [0.0]
+
+    def gc_cb(phase, info):
+        if phase == "start":
+            gc_t0[0] = _t.perf_counter()
+        else:
+            gc_log.append((info.get("generation", -1), _t.perf_counter() - gc_t0[0]))
+
+    gc.collect()
+    gc.freeze()
+    gc.callbacks.append(gc_cb)
     # saturation: every request present at t = 0 (median of 3 runs each)
     zero = np.zeros(len(picks))
     # warm-up: one whole untimed run (the first run grows the device's memory
@@ -921,6 +938,12 @@ def run_served(args, local_rank):
     lat_plain, _ = median_run(lambda: plain_fifo(arrivals),
                               key=lambda r: float(np.percentile(r[0], 99)))
     h.close()
+    gc.callbacks.remove(gc_cb)
+    gc.unfreeze()
+    gc_summary = {"collections": len(gc_log),
+                  "full_collections": sum(1 for g, _ in gc_log if g == 2),
+                  "pause_ms_total": round(sum(t for _, t in gc_log) * 1e3, 2),
+                  "pause_ms_max": round(max((t for _, t in gc_log), default=0.0) * 1e3, 2)}
     s_load = latency_summary(reqs_load)
     by_kind = {name: latency_summary([r for r, k in zip(reqs_load, kinds) if k == i])
                for i, name in enumerate(["small", "medium", "large"]) if (kinds == i).any()}
@@ -947,6 +970,7 @@ def run_served(args, local_rank):
                        "served_gflops": 2.0 * total_nip / span_sat / 1e9,
                        "batches": batches_sat,
                        "runs": spans[1:4]},
+        "python_gc": gc_summary,
         "at_load": {"offered_per_s": rate, "served": s_load, "served_by_kind": by_kind,
                     "plain_fifo_by_kind": plain_by_kind,
                     "plain_fifo": {"p50_ms": float(np.percentile(lat_plain, 50) * 1e3),

@@ -296,9 +296,14 @@ def pack_batch(pairs) -> PackedBatch:
         return rpt, col, val
 
     ar, ac, av = pack(As, b_row)
-    br, bc, bv = pack(Bs, c_col)
     A = DeviceCSR(int(a_row[-1]), int(b_row[-1]), ar, ac, av)
-    B = DeviceCSR(int(b_row[-1]), int(c_col[-1]), br, bc, bv)
+    if all(a is b for a, b in pairs) and np.array_equal(b_row, c_col):
+        # C_i = A_i * A_i with square A_i: the packed B is the packed A (same
+        # rows, same column shifts), so it is packed once
+        B = A
+    else:
+        br, bc, bv = pack(Bs, c_col)
+        B = DeviceCSR(int(b_row[-1]), int(c_col[-1]), br, bc, bv)
     return PackedBatch(a_row, b_row, c_col, A, B)
 
 
