@@ -253,9 +253,12 @@ class PackedBatch:
         return int(self.a_row_off.shape[0] - 1)
 
 
-def pack_batch(pairs) -> PackedBatch:
+def pack_batch(pairs, share: bool = False) -> PackedBatch:
     """Pack [(A_i, B_i)] (DeviceCSR, A_i.n == B_i.m) into block-diagonal operands
-    on the operands' device (host logic plus torch ops; no library call)."""
+    on the operands' device (host logic plus torch ops; no library call).
+    share: when every pair is one square matrix times itself, the packed B IS
+    the packed A (packed once) -- only for callers that do not update the
+    packed operands' values afterwards, as a plan over the batch does."""
     if torch is None:
         raise RuntimeError("torch is required")
     if not pairs:
@@ -297,7 +300,7 @@ def pack_batch(pairs) -> PackedBatch:
 
     ar, ac, av = pack(As, b_row)
     A = DeviceCSR(int(a_row[-1]), int(b_row[-1]), ar, ac, av)
-    if all(a is b for a, b in pairs) and np.array_equal(b_row, c_col):
+    if share and all(a is b for a, b in pairs) and np.array_equal(b_row, c_col):
         # C_i = A_i * A_i with square A_i: the packed B is the packed A (same
         # rows, same column shifts), so it is packed once
         B = A

@@ -507,7 +507,10 @@ struct EscCtaLayout {
     static_assert(bytes <= 232448, "an ESC CTA bin's shared memory exceeds 227 KB");
 };
 
-template<typename V, int THREADS, int NMAX>
+// SKIP_LE > 0: rows of at most SKIP_LE products are left to a smaller kernel
+// of the same bin; SKIP_GT: rows of more than NMAX products are left to a
+// larger one (instead of being reported).
+template<typename V, int THREADS, int NMAX, int SKIP_LE = 0, bool SKIP_GT = false>
 __global__ __launch_bounds__(THREADS) void k_esc_cta(ProductArgs p) {
     using L = EscCtaLayout<V, THREADS, NMAX>;
     constexpr int SHIFT = L::SHIFT;
@@ -523,6 +526,7 @@ __global__ __launch_bounds__(THREADS) void k_esc_cta(ProductArgs p) {
     const int row = p.rows[blockIdx.x];
     const int c0 = p.c_rpt[row];
     const int nip = p.c_rpt[row + 1] - c0;  // the row's NIP-sized slot
+    if (nip <= SKIP_LE || (SKIP_GT && nip > NMAX && p.row_nnz != nullptr)) return;
     if (nip > NMAX || p.row_nnz == nullptr) {
         if (tid == 0) report(p.status, kStCapacity, row, nip);
         return;
@@ -1135,6 +1139,23 @@ cudaError_t launch_esc_cta(const ProductArgs& p, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// The 256-thread ESC bin split by row size: rows of more than kEscCtaSmall
+// products with 256 threads, the others with 128 (half the fixed cost of each
+// radix pass and scan, twice the CTAs per SM).  Both grids cover the whole
+// row list; a CTA whose row belongs to the other kernel returns at once.
+// (1M power-law product: the bin 0.233 -> 0.223 ms serialised.)
+constexpr int kEscCtaSmall = 1024;
+
+template<typename V>
+cudaError_t launch_esc_cta_split(const ProductArgs& p, cudaStream_t s) {
+    k_esc_cta<V, 256, 3072, kEscCtaSmall, false>
+        <<<p.nrows, 256, EscCtaLayout<V, 256, 3072>::bytes, s>>>(p);
+    if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return e;
+    k_esc_cta<V, 128, kEscCtaSmall, 0, true>
+        <<<p.nrows, 128, EscCtaLayout<V, 128, kEscCtaSmall>::bytes, s>>>(p);
+    return cudaGetLastError();
+}
+
 template<typename V, int THREADS, int T, int CAP>
 cudaError_t launch_cta(const ProductArgs& p, cudaStream_t s) {
     k_s2n_cta<V, THREADS, T, CAP>
@@ -1339,7 +1360,7 @@ struct S2nEscLadder {
         {BinKind::Team, 768, 8, 256, EscLayout<V, 32, 256, 768>::bytes, "esc_team32_n768",    \
          launch_esc<V, 32, 256, 768>},                                                        \
         {BinKind::Cta, 3072, 1, 256, EscCtaLayout<V, 256, 3072>::bytes, "esc_cta256_n3072",    \
-         launch_esc_cta<V, 256, 3072>},                                                       \
+         launch_esc_cta_split<V>},                                                            \
         S2nBitmapLadder<V>::entries[5], S2nBitmapLadder<V>::entries[6],                       \
     };                                                                                        \
     template<>                                                                                \
@@ -1381,6 +1402,8 @@ cudaError_t prepare_one() {
     B200_SMEM((k_esc_team<V, 32, 256, 768>), (EscLayout<V, 32, 256, 768>::bytes));
     B200_SMEM((k_esc_team<V, 32, 256, kEscSplit>), (EscLayout<V, 32, 256, kEscSplit>::bytes));
     B200_SMEM((k_esc_cta<V, 256, 3072>), (EscCtaLayout<V, 256, 3072>::bytes));
+    B200_SMEM((k_esc_cta<V, 256, 3072, kEscCtaSmall, false>), (EscCtaLayout<V, 256, 3072>::bytes));
+    B200_SMEM((k_esc_cta<V, 128, kEscCtaSmall, 0, true>), (EscCtaLayout<V, 128, kEscCtaSmall>::bytes));
 #undef B200_SMEM
     return e;
 }

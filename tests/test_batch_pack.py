@@ -49,19 +49,21 @@ def test_pack_rejects_bad_pairs():
 
 
 def test_pack_square_self_products_once():
-    """C_i = A_i * A_i with square A_i: the packed B is the packed A itself,
-    equal to the block diagonal of the A_i; a non-square or distinct B is
-    packed on its own."""
+    """C_i = A_i * A_i with square A_i, share=True: the packed B is the packed A
+    itself, equal to the block diagonal of the A_i; without share (the
+    default: a plan may update the packed values) or with distinct operands B
+    is packed on its own."""
     from gpuspgemm_b200.api import pack_batch
     As = [G.power_law(200 + 40 * i, 2.0, 20, seed=30 + i) for i in range(4)]
     ds = [_dev(a) for a in As]
-    pb = pack_batch([(d, d) for d in ds])
+    assert pack_batch([(d, d) for d in ds]).B is not pack_batch([(d, d) for d in ds]).A
+    pb = pack_batch([(d, d) for d in ds], share=True)
     assert pb.B is pb.A
     R = sp.block_diag([_sp(M) for M in As], format="csr")
     assert np.array_equal(pb.B.rpt.numpy(), R.indptr)
     assert np.array_equal(pb.B.col.numpy(), R.indices)
     # the same operands given as distinct objects: packed twice, same arrays
-    pb2 = pack_batch([(d, _dev(a)) for d, a in zip(ds, As)])
+    pb2 = pack_batch([(d, _dev(a)) for d, a in zip(ds, As)], share=True)
     assert pb2.B is not pb2.A
     assert np.array_equal(pb2.B.col.numpy(), pb.A.col.numpy())
     # a rectangular A_i: B keeps its own column shifts
