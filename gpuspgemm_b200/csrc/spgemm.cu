@@ -99,6 +99,7 @@ struct spgemm_handle_s {
     cudaStream_t side[b200::kMaxSide] = {};
     cudaEvent_t ev_fork = nullptr;
     cudaEvent_t ev_sample = nullptr;  // the compression sample's side stream is done
+    cudaEvent_t ev_mirror = nullptr;  // the scratch front's copy to the host is done
     cudaEvent_t ev_join[b200::kMaxSide] = {};
     int nside = 4;
     // scratch (grown, never shrunk)
@@ -297,6 +298,35 @@ spgemm_status status_to_error(const DevStatus& st) {
 // The status word, both plans, the fail counter and the sample sit at the
 // front of the handle's scratch (ensure_scratch): one copy brings them all
 // back, and the host picks the words it asked for out of it.
+// The host's copy of the scratch front (plans, sample sums, status words)
+// in two halves: mirror_start queues the copy and an event behind the work
+// that wrote them, so later work can be queued before the host waits;
+// mirror_finish waits for that event only and unpacks the copy.
+spgemm_status mirror_start(spgemm_handle_s* h, cudaStream_t stream, const Scratch& s) {
+    const char* dev0 = static_cast<const char*>(h->scratch);
+    const size_t front = static_cast<size_t>(reinterpret_cast<const char*>(s.hist1) - dev0);
+    if (front > kFrontBytes) return fail(SPGEMM_ERR_INTERNAL, "scratch front exceeds its mirror");
+    B200_TRY(cudaMemcpyAsync(h->front_host, h->scratch, front, cudaMemcpyDeviceToHost, stream));
+    B200_TRY(cudaEventRecord(h->ev_mirror, stream));
+    return SPGEMM_OK;
+}
+
+spgemm_status mirror_finish(spgemm_handle_s* h, const Plan* plan, const Scratch& s,
+                            bool with_sample = false, const Plan* plan_b = nullptr) {
+    const char* dev0 = static_cast<const char*>(h->scratch);
+    B200_TRY(cudaEventSynchronize(h->ev_mirror));
+    h->info.host_syncs++;
+    auto at = [&](const void* dev) {
+        return h->front_host + (static_cast<const char*>(dev) - dev0);
+    };
+    std::memcpy(&h->mirror->plan, at(plan), sizeof(Plan));
+    if (plan_b != nullptr) std::memcpy(&h->mirror->plan_b, at(plan_b), sizeof(Plan));
+    if (with_sample) std::memcpy(&h->mirror->sample, at(s.sample), sizeof(EscSample));
+    std::memcpy(&h->mirror->status, at(s.status), sizeof(DevStatus));
+    std::memcpy(&h->mirror->fail_count, at(s.fail_count), sizeof(int32_t));
+    return SPGEMM_OK;
+}
+
 spgemm_status sync_mirror(spgemm_handle_s* h, cudaStream_t stream, const Plan* plan,
                           const Scratch& s, bool with_sample = false,
                           const Plan* plan_b = nullptr) {
@@ -606,6 +636,7 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         }
     }
     const bool nip_counts_fill = early && ladx_ok;
+    bool mirror_pending = false;  // mirror_start ran: the first wait is on its event
     B200_STEP(timed(h, "nip_hist", 0, -1, m, stream, [&](cudaStream_t ss) {
         return launch_nip_hist(A->rpt, A->col, B->rpt, m, c_rpt, off, s.hist1, s.plan1, s.status,
                                lad1, ss, s.hist3, s.cta_sum, nip_counts_fill ? &ladx : nullptr);
@@ -619,6 +650,11 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
                 return launch_bin_offsets_map(s.hist3, s.hist2, nctas, ladx, s.cta_sum, s.plan2,
                                               ladh, dlad, ss);
             }));
+            // everything the host decides on is final here (the NIP pass's
+            // plan, the fill plan, the sample, the status): its copy goes
+            // ahead of the scatter, which then overlaps the host's wait
+            B200_STEP_R(mirror_start(h, stream, s));
+            mirror_pending = true;
             B200_STEP_R(timed(h, "nip_fill_scatter", 2, -1, m, stream, [&](cudaStream_t ss) {
                 return launch_bin_scatter(off, m, s.hist2, s.cta_sum, s.bins2, s.plan2, ladh, true,
                                           ss, dlad, true);
@@ -663,7 +699,11 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         B200_STEP(count_binning());
     }
     mark(0);
-    B200_STEP(sync_mirror(h, stream, s.plan1, s, early && sampled, early ? s.plan2 : nullptr));
+    if (mirror_pending) {
+        B200_STEP(mirror_finish(h, s.plan1, s, early && sampled, early ? s.plan2 : nullptr));
+    } else {
+        B200_STEP(sync_mirror(h, stream, s.plan1, s, early && sampled, early ? s.plan2 : nullptr));
+    }
     mark(1);
     B200_STEP(status_to_error(h->mirror->status));
     Plan p1 = h->mirror->plan;  // bin sizes valid once the count binning ran
@@ -1995,6 +2035,7 @@ spgemm_status spgemm_create(spgemm_handle_t* handle, int device) {
     }
     B200_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     B200_TRY(cudaEventCreateWithFlags(&h->ev_sample, cudaEventDisableTiming));
+    B200_TRY(cudaEventCreateWithFlags(&h->ev_mirror, cudaEventDisableTiming));
     B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&h->mirror), sizeof(HostMirror)));
     B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&h->front_host), kFrontBytes));
     if (spgemm_status st = device_pool(dev, &h->pool); st != SPGEMM_OK) return st;
@@ -2012,6 +2053,7 @@ spgemm_status spgemm_destroy(spgemm_handle_t h) {
     }
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_sample) cudaEventDestroy(h->ev_sample);
+    if (h->ev_mirror) cudaEventDestroy(h->ev_mirror);
     if (h->scratch) cudaFree(h->scratch);
     if (h->bitmaps) cudaFree(h->bitmaps);
     if (h->onepass) cudaFree(h->onepass);
