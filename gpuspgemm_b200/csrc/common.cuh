@@ -29,7 +29,8 @@ enum : unsigned {
     kStBadInput = 4u,     // checked mode found an invalid operand
     kStNipOverflow = 8u,  // a row's NIP does not fit int32
     kStClusterFail = 16u, // (diagnostic) a cluster row spilled to the global bin
-    kStIndex = 32u        // a computed shared-memory index or alignment failed its check
+    kStIndex = 32u,       // a computed shared-memory index or alignment failed its check
+    kStWait = 64u         // a bounded wait on another CTA's result ran out
 };
 
 struct DevStatus {

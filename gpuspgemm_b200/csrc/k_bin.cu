@@ -451,95 +451,124 @@ __global__ __launch_bounds__(kBinThreads) void k_bin_scatter(
     }
 }
 
-// ---- one-pass row pointer: reduce, then scan --------------------------------
-// The rows' nnz become the row pointer in two launches: k_rpt_reduce sums (and
-// maxes) each tile of kScanTile counts; k_rpt_scan adds the sums of the tiles
-// before its own (read by each CTA itself) to an in-place exclusive scan of
-// its tile.  12 bytes of traffic per row, where a one-bin pass of the binning
+// ---- one-pass row pointer -----------------------------------------------------
+// The rows' nnz become the row pointer in place, tile by tile (kScanTile rows
+// a CTA): 8 bytes of traffic per row, where a one-bin pass of the binning
 // kernels takes three launches and also writes a row list.
 constexpr int kScanThreads = 256;
 constexpr int kScanPer = kScanTile / kScanThreads;  // rows per thread
 static_assert(kScanPer * kScanThreads == kScanTile, "tile");
 
-__global__ __launch_bounds__(kScanThreads) void k_rpt_reduce(const int32_t* __restrict__ cnt,
-                                                             int32_t m,
-                                                             int64_t* __restrict__ tile_sum,
-                                                             Plan* __restrict__ plan) {
-    __shared__ long long s_sum[kScanThreads / kWarp];
-    __shared__ int32_t s_max[kScanThreads / kWarp];
-    const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int w = tid >> 5;
-    const long long r0 = static_cast<long long>(blockIdx.x) * kScanTile;
-    long long sum = 0;
-    int32_t mx = 0;
-#pragma unroll
-    for (int k = 0; k < kScanPer; k++) {
-        const long long r = r0 + k * kScanThreads + tid;
-        if (r < m) {
-            const int32_t v = cnt[r];
-            sum += v;
-            mx = max(mx, v);
-        }
-    }
-    sum = warp_sum_ll(sum);
-    mx = __reduce_max_sync(0xffffffffu, mx);
-    if (lane == 0) {
-        s_sum[w] = sum;
-        s_max[w] = mx;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        long long t = 0;
-        int32_t x = 0;
-        for (int i = 0; i < kScanThreads / kWarp; i++) {
-            t += s_sum[i];
-            x = max(x, s_max[i]);
-        }
-        tile_sum[blockIdx.x] = t;
-        atomicMax(&plan->max_key, x);
-    }
-}
-
 // the tile in shared memory, one padding word per 32 (thread t reads its
 // kScanPer consecutive rows without bank conflicts)
 __device__ __forceinline__ int scan_pad(int i) { return i + (i >> 5); }
 
-__global__ __launch_bounds__(kScanThreads) void k_rpt_scan(int32_t* __restrict__ cnt, int32_t m,
-                                                           const int64_t* __restrict__ tile_sum,
-                                                           Plan* __restrict__ plan) {
+// One launch, the tiles chained by decoupled look-back.
+// Each CTA takes the next tile from a ticket counter (state[0]), so every tile
+// before its own belongs to a CTA that has already started; it scans its tile
+// in shared memory and publishes the tile's sum in state[1 + tile].  Warp 0
+// then reads the states of the tiles before it, 32 at a time, adding their
+// sums back to the nearest tile that has published its prefix (the sum of the
+// counts through that tile), and publishes its own prefix.  A state word holds
+// its kind in the top two bits (0: nothing yet, kTileSum, kTilePrefix) and the
+// value below them; the counter and states are zeroed before the launch.  The
+// waits are bounded: past kLookbackSpins rounds the CTA reports kStWait and
+// goes on with what it has, and the call fails on the status.  (It replaced a
+// reduce launch plus a scan launch: 1M rows 0.021 -> 0.011 ms.)
+constexpr unsigned long long kTileSum = 1ull << 62;
+constexpr unsigned long long kTilePrefix = 2ull << 62;
+constexpr unsigned long long kTileValue = (1ull << 62) - 1ull;
+constexpr int kLookbackSpins = 1 << 20;
+
+__global__ __launch_bounds__(kScanThreads) void k_rpt_scan1(int32_t* __restrict__ cnt, int32_t m,
+                                                            int32_t ntiles,
+                                                            unsigned long long* __restrict__ state,
+                                                            Plan* __restrict__ plan,
+                                                            DevStatus* __restrict__ st) {
+    constexpr int NW = kScanThreads / kWarp;
+    constexpr unsigned kAll = 0xffffffffu;
     __shared__ int32_t s_row[kScanTile + kScanTile / 32];
-    __shared__ long long s_before[kScanThreads / kWarp];
-    __shared__ int32_t s_wtot[kScanThreads / kWarp];
+    __shared__ int32_t s_wtot[NW];
+    __shared__ int32_t s_wmax[NW];
+    __shared__ int32_t s_tile;
+    __shared__ long long s_base;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int w = tid >> 5;
-    // the counts of the tiles before this one
-    long long before = 0;
-    for (int t = tid; t < static_cast<int>(blockIdx.x); t += kScanThreads) before += tile_sum[t];
-    before = warp_sum_ll(before);
-    if (lane == 0) s_before[w] = before;
-    const long long r0 = static_cast<long long>(blockIdx.x) * kScanTile;
+    if (tid == 0) s_tile = static_cast<int32_t>(atomicAdd(state, 1ull));
+    __syncthreads();
+    const int tile = s_tile;
+    if (tile >= ntiles) {  // a counter left from an earlier launch: uniform over the CTA
+        if (tid == 0) report(st, kStIndex, tile, ntiles);
+        return;
+    }
+    const long long r0 = static_cast<long long>(tile) * kScanTile;
 #pragma unroll
     for (int k = 0; k < kScanPer; k++) {
         const int j = k * kScanThreads + tid;
         s_row[scan_pad(j)] = r0 + j < m ? cnt[r0 + j] : 0;
     }
     __syncthreads();
-    long long base = 0;
-#pragma unroll
-    for (int i = 0; i < kScanThreads / kWarp; i++) base += s_before[i];
-    // thread tid: rows [tid * kScanPer, (tid + 1) * kScanPer) of the tile.
-    // int arithmetic inside the tile: it wraps only when the total leaves
-    // int32, which the plan's int64 total flags
+    // thread tid: rows [tid * kScanPer, (tid + 1) * kScanPer) of the tile
     int v[kScanPer];
     int run = 0;
+    int mx = 0;
 #pragma unroll
     for (int k = 0; k < kScanPer; k++) {
         v[k] = s_row[scan_pad(tid * kScanPer + k)];
         run += v[k];
+        mx = max(mx, v[k]);
     }
+    mx = __reduce_max_sync(kAll, mx);
+    if (lane == 0) s_wmax[w] = mx;
     const int inc = block_inclusive_scan<kScanThreads>(run, s_wtot);
+    __syncthreads();
+    if (w == 0) {
+        const long long tsum = static_cast<unsigned>(s_wtot[NW - 1]);  // counts: >= 0
+        int tmax = lane < NW ? s_wmax[lane] : 0;
+        tmax = __reduce_max_sync(kAll, tmax);
+        if (lane == 0) {
+            atomicMax(&plan->max_key, tmax);
+            atomicExch(state + 1 + tile, (tile == 0 ? kTilePrefix : kTileSum) |
+                                             min(static_cast<unsigned long long>(tsum), kTileValue));
+        }
+        long long excl = 0;
+        int pred = tile - 1;
+        int spins = 0;
+        while (pred >= 0) {
+            const int t = pred - lane;
+            const unsigned long long f =
+                t >= 0 ? static_cast<unsigned long long>(
+                             *reinterpret_cast<volatile unsigned long long*>(state + 1 + t))
+                       : kTilePrefix;
+            const unsigned kind = static_cast<unsigned>(f >> 62);
+            const unsigned pre = __ballot_sync(kAll, kind == 2u);
+            // the lanes up to the nearest prefix (all 32 when there is none)
+            const unsigned upto = pre != 0u ? ((pre & (0u - pre)) << 1) - 1u : kAll;
+            if ((__ballot_sync(kAll, kind == 0u) & upto) != 0u) {
+                if (++spins > kLookbackSpins) {
+                    if (lane == 0) report(st, kStWait, tile, pred);
+                    break;
+                }
+                __nanosleep(32);
+                continue;
+            }
+            const long long x = (upto >> lane) & 1u ? static_cast<long long>(f & kTileValue) : 0;
+            excl += warp_sum_ll(x);
+            if (pre != 0u) break;
+            pred -= kWarp;
+        }
+        if (lane == 0) {
+            if (tile > 0)
+                atomicExch(state + 1 + tile,
+                           kTilePrefix | min(static_cast<unsigned long long>(excl + tsum), kTileValue));
+            s_base = excl;
+        }
+    }
+    __syncthreads();
+    const long long base = s_base;
+    // int arithmetic inside the tile: it wraps only when the total leaves
+    // int32, which the plan's int64 total flags
     int pos = static_cast<int>(base) + inc - run;
 #pragma unroll
     for (int k = 0; k < kScanPer; k++) {
@@ -552,8 +581,8 @@ __global__ __launch_bounds__(kScanThreads) void k_rpt_scan(int32_t* __restrict__
         const int j = k * kScanThreads + tid;
         if (r0 + j < m) cnt[r0 + j] = s_row[scan_pad(j)];
     }
-    if (blockIdx.x == gridDim.x - 1 && tid == 0) {
-        const long long total = base + s_wtot[kScanThreads / kWarp - 1];
+    if (tile == ntiles - 1 && tid == 0) {
+        const long long total = base + static_cast<unsigned>(s_wtot[NW - 1]);
         cnt[m] = static_cast<int32_t>(total);
         plan->total_key = total;
         plan->overflow = total > INT32_MAX ? 1 : 0;
@@ -703,17 +732,11 @@ cudaError_t launch_bin_offsets_map(const int32_t* src_hist, int32_t* hist, int32
     return cudaGetLastError();
 }
 
-cudaError_t launch_rpt_reduce(const int32_t* cnt, int32_t m, int64_t* tile_sum, Plan* plan,
-                              cudaStream_t s) {
+cudaError_t launch_rpt_scan1(int32_t* cnt, int32_t m, unsigned long long* state, Plan* plan,
+                             DevStatus* st, cudaStream_t s) {
     if (m <= 0) return cudaSuccess;
-    k_rpt_reduce<<<rpt_scan_tiles(m), kScanThreads, 0, s>>>(cnt, m, tile_sum, plan);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_rpt_scan(int32_t* cnt, int32_t m, const int64_t* tile_sum, Plan* plan,
-                            cudaStream_t s) {
-    if (m <= 0) return cudaSuccess;
-    k_rpt_scan<<<rpt_scan_tiles(m), kScanThreads, 0, s>>>(cnt, m, tile_sum, plan);
+    const int tiles = rpt_scan_tiles(m);
+    k_rpt_scan1<<<tiles, kScanThreads, 0, s>>>(cnt, m, tiles, state, plan, st);
     return cudaGetLastError();
 }
 

@@ -198,17 +198,17 @@ cudaError_t launch_bin_scatter(int32_t* c_rpt, int32_t m, const int32_t* hist_of
                                const Ladder& lad, bool scan, cudaStream_t s,
                                const Ladder* dlad = nullptr, bool bin_relative = false);
 // One-pass row pointer: rewrite cnt[0..m) (each row's nnz) as its exclusive
-// scan and cnt[m] as the total, in place; the plan (zeroed by the caller)
-// receives the total, the max and the int32 overflow flag.  tile_sum holds
-// rpt_scan_tiles(m) sums.  Only for rpt_scan_tiles(m) <= kScanMaxTiles (each
-// CTA adds up the tiles before its own).
+// scan and cnt[m] as the total, in place, in one launch (tiles chained by
+// decoupled look-back); the plan (zeroed by the caller) receives the total,
+// the max and the int32 overflow flag.  state holds 1 + rpt_scan_tiles(m)
+// zeroed words (a ticket counter, then one per tile); a look-back that waits
+// too long reports kStWait in st.  Used for rpt_scan_tiles(m) <=
+// kScanMaxTiles (the size of the state in the scratch).
 constexpr int kScanTile = 4096;
 constexpr int kScanMaxTiles = 2048;
 inline int rpt_scan_tiles(int32_t m) { return (m + kScanTile - 1) / kScanTile; }
-cudaError_t launch_rpt_reduce(const int32_t* cnt, int32_t m, int64_t* tile_sum, Plan* plan,
-                              cudaStream_t s);
-cudaError_t launch_rpt_scan(int32_t* cnt, int32_t m, const int64_t* tile_sum, Plan* plan,
-                            cudaStream_t s);
+cudaError_t launch_rpt_scan1(int32_t* cnt, int32_t m, unsigned long long* state, Plan* plan,
+                             DevStatus* st, cudaStream_t s);
 // One-pass fill: copy each row's entries from its slot [off[r], ...) of the
 // temporary arrays to [rpt[r], rpt[r+1]) of C (values of value_bytes 4 or 8);
 // nothing at or past `cap`, C's capacity.

@@ -57,6 +57,9 @@ constexpr int64_t kBitmapBudget = int64_t(1) << 30;
 struct Scratch {
     DevStatus* status;
     Plan* plan1;
+    // the one-pass row pointer's look-back: a ticket counter and one state per
+    // tile (behind the mirrored front)
+    unsigned long long* scan_state;
     Plan* plan2;
     int32_t* hist1;
     int32_t* hist2;
@@ -200,6 +203,7 @@ spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s, cudaStre
     const size_t o_bins2 = take(sizeof(int32_t) * mm);
     const size_t o_fail = take(sizeof(int32_t) * mm);
     const size_t o_work = take(sizeof(int32_t) * kMaxBins);
+    const size_t o_scan = take(sizeof(unsigned long long) * (1 + kScanMaxTiles));
     if (spgemm_status st = regrow(h, &h->scratch, &h->scratch_bytes, off + off / 4, stream);
         st != SPGEMM_OK)
         return st;
@@ -218,6 +222,7 @@ spgemm_status ensure_scratch(spgemm_handle_s* h, int32_t m, Scratch* s, cudaStre
     s->bins2 = reinterpret_cast<int32_t*>(b + o_bins2);
     s->fail_rows = reinterpret_cast<int32_t*>(b + o_fail);
     s->work = reinterpret_cast<int32_t*>(b + o_work);
+    s->scan_state = reinterpret_cast<unsigned long long*>(b + o_scan);
     return SPGEMM_OK;
 }
 
@@ -637,6 +642,10 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
     }
     const bool nip_counts_fill = early && ladx_ok;
     bool mirror_pending = false;  // mirror_start ran: the first wait is on its event
+    // the row pointer's look-back scan needs its ticket and tile states zeroed
+    const bool scan1 = rpt_scan_tiles(m) <= kScanMaxTiles;
+    const size_t scan_bytes = sizeof(unsigned long long) * (1 + size_t(rpt_scan_tiles(m)));
+    bool scan_zeroed = false;
     B200_STEP(timed(h, "nip_hist", 0, -1, m, stream, [&](cudaStream_t ss) {
         return launch_nip_hist(A->rpt, A->col, B->rpt, m, c_rpt, off, s.hist1, s.plan1, s.status,
                                lad1, ss, s.hist3, s.cta_sum, nip_counts_fill ? &ladx : nullptr);
@@ -655,6 +664,11 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
             // ahead of the scatter, which then overlaps the host's wait
             B200_STEP_R(mirror_start(h, stream, s));
             mirror_pending = true;
+            // (zeroed here, while the host waits on the mirror's event)
+            if (scan1) {
+                B200_TRY(cudaMemsetAsync(s.scan_state, 0, scan_bytes, stream));
+                scan_zeroed = true;
+            }
             B200_STEP_R(timed(h, "nip_fill_scatter", 2, -1, m, stream, [&](cudaStream_t ss) {
                 return launch_bin_scatter(off, m, s.hist2, s.cta_sum, s.bins2, s.plan2, ladh, true,
                                           ss, dlad, true);
@@ -850,15 +864,14 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
         mark(4);
         B200_ONE(launch_bins(h, one_fil, nfil, 3, pf, s.bins2, pa, stream));
         // row pointer from the counts, into the count binning's plan (reset:
-        // its max and overflow only ever grow): reduce, then scan -- or, past
-        // the scan's tile limit, a one-bin pass of the binning kernels
+        // its max and overflow only ever grow): one look-back scan -- or, past
+        // its tile limit, a one-bin pass of the binning kernels
         B200_ONE_CUDA(cudaMemsetAsync(s.plan1, 0, sizeof(Plan), stream), "reset a plan");
-        if (rpt_scan_tiles(m) <= kScanMaxTiles) {
-            B200_ONE(timed(h, "count_scan_reduce", 2, -1, m, stream, [&](cudaStream_t ss) {
-                return launch_rpt_reduce(c_rpt, m, s.cta_sum, s.plan1, ss);
-            }));
+        if (scan1 && !scan_zeroed)
+            B200_ONE_CUDA(cudaMemsetAsync(s.scan_state, 0, scan_bytes, stream), "reset the scan");
+        if (scan1) {
             B200_ONE(timed(h, "count_scan_rows", 2, -1, m, stream, [&](cudaStream_t ss) {
-                return launch_rpt_scan(c_rpt, m, s.cta_sum, s.plan1, ss);
+                return launch_rpt_scan1(c_rpt, m, s.scan_state, s.plan1, s.status, ss);
             }));
         } else {
             Ladder one = {};
