@@ -271,9 +271,13 @@ __device__ __forceinline__ int offmap_pad(int j) { return j + (j >> 5); }
 __global__ __launch_bounds__(kOffMapThreads) void k_bin_offsets_map(
     const int32_t* __restrict__ src_hist, int32_t* __restrict__ hist, int32_t nctas,
     const __grid_constant__ Ladder src, int64_t* __restrict__ cta_sum, Plan* __restrict__ plan,
-    const __grid_constant__ Ladder lad, const Ladder* __restrict__ dlad) {
+    const __grid_constant__ Ladder lad, const Ladder* __restrict__ dlad,
+    unsigned long long* __restrict__ zero, int32_t nzero) {
     constexpr int NW = kOffMapThreads / kWarp;
     constexpr int PADDED = kOffMapChunk + kOffMapChunk / kWarp;
+    // words a later kernel of the product needs zeroed (the row pointer's
+    // look-back state): cleared here instead of by a memset of their own
+    for (int i = threadIdx.x; i < nzero; i += kOffMapThreads) zero[i] = 0ull;
     static_assert(NW > kMaxBins, "a warp per bin and one for the CTA sums");
     static_assert(kBinRowsPerCta < 65536, "16-bit counts");
     __shared__ uint16_t s_cnt[kMaxBins][PADDED + 1];
@@ -726,9 +730,10 @@ cudaError_t launch_nip_hist(const int32_t* a_rpt, const int32_t* a_col, const in
 
 cudaError_t launch_bin_offsets_map(const int32_t* src_hist, int32_t* hist, int32_t nctas,
                                    const Ladder& src, int64_t* cta_sum, Plan* plan,
-                                   const Ladder& lad, const Ladder* dlad, cudaStream_t s) {
+                                   const Ladder& lad, const Ladder* dlad, cudaStream_t s,
+                                   unsigned long long* zero, int32_t nzero) {
     k_bin_offsets_map<<<1, kOffMapThreads, 0, s>>>(src_hist, hist, nctas, src, cta_sum, plan, lad,
-                                                   dlad);
+                                                   dlad, zero, nzero);
     return cudaGetLastError();
 }
 

@@ -178,10 +178,12 @@ cudaError_t launch_nip_hist(const int32_t* a_rpt, const int32_t* a_col, const in
 // limits include every limit of the final ladder (dlad when given, else lad):
 // the outputs of launch_bin_offsets for the final ladder, all bins at once,
 // except that hist (another array) receives offsets within each bin: the
-// scatter that reads them is launched with bin_relative.
+// scatter that reads them is launched with bin_relative.  It also zeroes
+// zero[0..nzero), words a later kernel needs cleared.
 cudaError_t launch_bin_offsets_map(const int32_t* src_hist, int32_t* hist, int32_t nctas,
                                    const Ladder& src, int64_t* cta_sum, Plan* plan,
-                                   const Ladder& lad, const Ladder* dlad, cudaStream_t s);
+                                   const Ladder& lad, const Ladder* dlad, cudaStream_t s,
+                                   unsigned long long* zero = nullptr, int32_t nzero = 0);
 // Pass 1' (key = nnz already in c_rpt): per-CTA sums and bin histograms.
 // dlad: limits chosen on the device (same bin count as lad), or nullptr.
 cudaError_t launch_nnz_hist(const int32_t* c_rpt, int32_t m, int32_t* hist, int64_t* cta_sum,

@@ -655,20 +655,18 @@ spgemm_status product(spgemm_handle_s* h, const spgemm_csr_view* A, const spgemm
             // the NIP pass counted the rows by ladx: offsets for the chosen
             // ladder, then the scatter
             if (sampled) B200_TRY(cudaStreamWaitEvent(stream, h->ev_sample, 0));
+            // (the row pointer's look-back state is zeroed by the same launch)
             B200_STEP_R(timed(h, "nip_fill_offsets", 2, -1, m, stream, [&](cudaStream_t ss) {
                 return launch_bin_offsets_map(s.hist3, s.hist2, nctas, ladx, s.cta_sum, s.plan2,
-                                              ladh, dlad, ss);
+                                              ladh, dlad, ss, scan1 ? s.scan_state : nullptr,
+                                              scan1 ? static_cast<int32_t>(scan_bytes / 8) : 0);
             }));
+            scan_zeroed = scan1;
             // everything the host decides on is final here (the NIP pass's
             // plan, the fill plan, the sample, the status): its copy goes
             // ahead of the scatter, which then overlaps the host's wait
             B200_STEP_R(mirror_start(h, stream, s));
             mirror_pending = true;
-            // (zeroed here, while the host waits on the mirror's event)
-            if (scan1) {
-                B200_TRY(cudaMemsetAsync(s.scan_state, 0, scan_bytes, stream));
-                scan_zeroed = true;
-            }
             B200_STEP_R(timed(h, "nip_fill_scatter", 2, -1, m, stream, [&](cudaStream_t ss) {
                 return launch_bin_scatter(off, m, s.hist2, s.cta_sum, s.bins2, s.plan2, ladh, true,
                                           ss, dlad, true);
