@@ -103,6 +103,7 @@ struct spgemm_handle_s {
     cudaEvent_t ev_fork = nullptr;
     cudaEvent_t ev_sample = nullptr;  // the compression sample's side stream is done
     cudaEvent_t ev_mirror = nullptr;  // the scratch front's copy to the host is done
+    cudaEvent_t ev_front = nullptr;   // the scratch front is final (the copy may start)
     cudaEvent_t ev_join[b200::kMaxSide] = {};
     int nside = 4;
     // scratch (grown, never shrunk)
@@ -306,13 +307,19 @@ spgemm_status status_to_error(const DevStatus& st) {
 // The host's copy of the scratch front (plans, sample sums, status words)
 // in two halves: mirror_start queues the copy and an event behind the work
 // that wrote them, so later work can be queued before the host waits;
-// mirror_finish waits for that event only and unpacks the copy.
+// mirror_finish waits for that event only and unpacks the copy.  The copy
+// runs on the last side stream (behind an event on `stream`), so the work
+// queued on `stream` after it does not wait for it; that work must not write
+// the front.
 spgemm_status mirror_start(spgemm_handle_s* h, cudaStream_t stream, const Scratch& s) {
     const char* dev0 = static_cast<const char*>(h->scratch);
     const size_t front = static_cast<size_t>(reinterpret_cast<const char*>(s.hist1) - dev0);
     if (front > kFrontBytes) return fail(SPGEMM_ERR_INTERNAL, "scratch front exceeds its mirror");
-    B200_TRY(cudaMemcpyAsync(h->front_host, h->scratch, front, cudaMemcpyDeviceToHost, stream));
-    B200_TRY(cudaEventRecord(h->ev_mirror, stream));
+    cudaStream_t copy = h->side[kMaxSide - 1];
+    B200_TRY(cudaEventRecord(h->ev_front, stream));
+    B200_TRY(cudaStreamWaitEvent(copy, h->ev_front, 0));
+    B200_TRY(cudaMemcpyAsync(h->front_host, h->scratch, front, cudaMemcpyDeviceToHost, copy));
+    B200_TRY(cudaEventRecord(h->ev_mirror, copy));
     return SPGEMM_OK;
 }
 
@@ -2047,6 +2054,7 @@ spgemm_status spgemm_create(spgemm_handle_t* handle, int device) {
     B200_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     B200_TRY(cudaEventCreateWithFlags(&h->ev_sample, cudaEventDisableTiming));
     B200_TRY(cudaEventCreateWithFlags(&h->ev_mirror, cudaEventDisableTiming));
+    B200_TRY(cudaEventCreateWithFlags(&h->ev_front, cudaEventDisableTiming));
     B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&h->mirror), sizeof(HostMirror)));
     B200_TRY(cudaMallocHost(reinterpret_cast<void**>(&h->front_host), kFrontBytes));
     if (spgemm_status st = device_pool(dev, &h->pool); st != SPGEMM_OK) return st;
@@ -2065,6 +2073,7 @@ spgemm_status spgemm_destroy(spgemm_handle_t h) {
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_sample) cudaEventDestroy(h->ev_sample);
     if (h->ev_mirror) cudaEventDestroy(h->ev_mirror);
+    if (h->ev_front) cudaEventDestroy(h->ev_front);
     if (h->scratch) cudaFree(h->scratch);
     if (h->bitmaps) cudaFree(h->bitmaps);
     if (h->onepass) cudaFree(h->onepass);
