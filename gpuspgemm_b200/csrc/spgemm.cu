@@ -296,6 +296,13 @@ spgemm_status status_to_error(const DevStatus& st) {
                       st.row, st.detail);
         return fail(SPGEMM_ERR_INVALID_ARG, buf);
     }
+    if (st.flags & kStWait) {
+        std::snprintf(buf, sizeof buf,
+                      "a bounded device wait ran out (the row pointer's look-back: tile %d "
+                      "waiting on tile %d or one of the 31 before it)",
+                      st.row, st.detail);
+        return fail(SPGEMM_ERR_TIMEOUT, buf);
+    }
     std::snprintf(buf, sizeof buf, "device status 0x%x at row %d (detail %d)", st.flags, st.row,
                   st.detail);
     return fail(SPGEMM_ERR_INTERNAL, buf);
